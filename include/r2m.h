@@ -1,0 +1,171 @@
+/*
+ * r2m.h -- C ABI of librotormap_b200.so, the B200 (sm_100a) read-mapping hot
+ * path of RotorMap: rope encode -> fp8 read x index GEMM -> per-row top-k.
+ *
+ * Conventions (every entry point):
+ *   - return 0 on success, a negative R2M_E* code on failure; the message of
+ *     the last failure on the calling thread is r2m_last_error();
+ *   - device pointers are plain CUDA device addresses owned by the caller;
+ *     an engine owns only its own workspace;
+ *   - `stream` is a cudaStream_t (NULL = the legacy default stream); every
+ *     device call is stream-ordered and returns without synchronizing;
+ *   - index conventions follow the reference: global column ids are 1-based,
+ *     0 marks an empty slot whose value is -Inf.
+ *
+ * Each declaration names the reference function it replaces (file:line in
+ * q4bio-qpg/qpg-rotormap, RotorMap/ tree).
+ */
+#ifndef R2M_H
+#define R2M_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *r2m_stream_t; /* cudaStream_t */
+
+enum {
+  R2M_OK = 0,
+  R2M_EINVAL = -1,   /* bad argument (shape, alignment, range) */
+  R2M_ECUDA = -2,    /* a CUDA runtime/driver call failed */
+  R2M_ENOMEM = -3,   /* device or host allocation failed */
+  R2M_ETIMEOUT = -4, /* a bounded device-side wait gave up (kernel aborted) */
+  R2M_ESTATE = -5,   /* wrong object state (e.g. no device, not initialised) */
+  R2M_EIO = -6       /* host input could not be read/parsed */
+};
+
+/* Output element kinds of the encoders. */
+enum {
+  R2M_OUT_F32 = 0,        /* fp32 [Re; Im] rows (the kernel's compute type) */
+  R2M_OUT_F16 = 1,        /* fp16 RNE rows (the reference stream's fp16 = true) */
+  R2M_OUT_E4M3 = 2,       /* e4m3(fp32(fp16(x))): the reference's quantisation, scale 1 */
+  R2M_OUT_E4M3_SCALED = 3 /* e4m3(x * 448/amax_row) + fp32 row scale amax_row/448 */
+};
+
+/* Score semantics of the fused GEMM + top-k. */
+enum {
+  R2M_SCORE_F16 = 0,   /* fp32 accumulate, rounded to fp16 (reference cout = :f16) */
+  R2M_SCORE_F32 = 1,   /* fp32 accumulate, unrounded (reference cout = :f32) */
+  R2M_SCORE_SCALED = 2 /* fp32 accumulate x scaleA[row] x scaleB[col] (per-row scales) */
+};
+
+/* Library identity and last error (thread-local). */
+const char *r2m_last_error(void);
+int r2m_version(void);
+/* 0 when a CUDA device of compute capability 10.x is current, else an error. */
+int r2m_device_check(void);
+/* Synchronizes `stream`, then reports (R2M_ETIMEOUT) and clears a bounded
+ * device-side wait that gave up in a kernel of this library since the last
+ * check on the current device.  No reference counterpart: the reference's
+ * kernels have no bounded waits. */
+int r2m_check_device_error(r2m_stream_t stream);
+
+/* ---------------------------------------------------------------- encode */
+
+/* Replaces encode_frag_real_batch! (RotorMap/encode/kernel.jl:298-325) and
+ * the kernel kernel_rope_frag_real (kernel.jl:86-290).
+ * dnas: n * cld(k,16) forward 2-bit words (base j at word j>>4, bits
+ * 2*(j&15), zero-padded tail).  dest: (n, 2*m*4^c) row-major of `out_kind`
+ * ([Re; Im] split layout).  dest_norms: (n, m) fp32 (row = fragment), the
+ * reference's embeds_norms column per fragment.  dest_scales: n fp32 row
+ * scales, required for R2M_OUT_E4M3_SCALED, ignored otherwise (may be NULL).
+ * normalize in 0..3.  Requires s <= 16, c <= s, 1 <= m <= 8, k >= s. */
+int r2m_encode_frag_real_batch(void *dest, int out_kind, float *dest_norms,
+                               float *dest_scales, const uint32_t *dnas,
+                               int64_t n, int k, int s, int m, int c,
+                               int normalize, r2m_stream_t stream);
+
+/* Replaces revcomp_frag_words! / kernel_revcomp_words!
+ * (RotorMap/index/build.jl:448-476): drc = reverse complement of each
+ * fragment's k bases, forward-packed with a zero tail. */
+int r2m_revcomp_frag_words(uint32_t *drc, const uint32_t *dnas, int k,
+                           int64_t n, r2m_stream_t stream);
+
+/* Replaces the index builder's encode step (ref_rope_real_stream +
+ * build_index_matrix, RotorMap/index/build.jl:547-749): encodes the
+ * forward and reverse-complement k-window of every window start into index
+ * columns.  genome: packed 2-bit words of all records (each record starting
+ * at a word boundary, followed by at least one zero guard word);
+ * win_pos[i] = absolute base position (16 * record word offset + 0-based
+ * window offset) of window i.  Column layout is the reference's: windows are
+ * grouped in batches of `batch_size`; batch b (nb windows) fills columns
+ * [2*b*batch_size, 2*b*batch_size + nb) with forward windows and the next nb
+ * columns with their reverse complements.  dest: (2*nwin, 2*m*4^c) rows of
+ * `out_kind`; dest_norms (2*nwin, m); dest_scales 2*nwin (SCALED only). */
+int r2m_encode_ref_windows(void *dest, int out_kind, float *dest_norms,
+                           float *dest_scales, const uint32_t *genome,
+                           const int64_t *win_pos, int64_t nwin,
+                           int64_t batch_size, int k, int s, int m, int c,
+                           int normalize, r2m_stream_t stream);
+
+/* Replaces f32_to_f8! (RotorMap/gemm/fp8_convert.jl:100,
+ * fp8_ptx.jl:161-166) and the fp16 -> fp32 -> e4m3 step of
+ * upload_fp16_as_f8! (RotorMap/search/engine_fp8.jl:355-371):
+ * cvt.rn.satfinite e4m3, element-wise over `count` values. */
+int r2m_f32_to_e4m3(uint8_t *dst, const float *src, int64_t count,
+                    r2m_stream_t stream);
+int r2m_f16_to_e4m3(uint8_t *dst, const uint16_t *src, int64_t count,
+                    r2m_stream_t stream);
+
+/* ---------------------------------------------------------------- search */
+
+typedef struct r2m_engine r2m_engine;
+
+/* Schedule knobs of the fused GEMM + top-k (0 = automatic). */
+typedef struct {
+  int splits;  /* column splits per read tile (k-split of the top-k) */
+  int ctas;    /* persistent CTAs (default: SM count) */
+  int reserved[6];
+} r2m_tuning;
+
+/* Replaces TopKEngine(B; k, w, rows_cap, segs, engine, cout)
+ * (RotorMap/search/engine_fp8.jl:309-337).  d_B: the resident e4m3 index,
+ * N columns of rdim bytes each (the reference's (rdim, N) column-major
+ * embeds8; 16-byte aligned).  d_scaleB: N fp32 column scales
+ * (R2M_SCORE_SCALED only, else NULL).  rows_cap: largest batch height.
+ * 1 <= k <= min(N, 64); rdim % 16 == 0. */
+int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int rdim,
+                      int64_t N, int k, int rows_cap, int score_mode,
+                      const r2m_tuning *tune, r2m_engine **out);
+int r2m_engine_destroy(r2m_engine *eng);
+/* Bytes of device workspace the engine holds. */
+int64_t r2m_engine_workspace_bytes(const r2m_engine *eng);
+
+/* Replaces batch_gemm_topk! (RotorMap/search/engine_fp8.jl:399-437) with the
+ * cuBLASLt GEMM (fp8_lt.jl:128-168) and seg_rowtopk_merge_kernel!
+ * (gemm/topk_kernels.jl:213-329) fused into one tcgen05 kernel plus a
+ * split-merge kernel; the score matrix never reaches HBM.
+ * d_A: nb rows of rdim e4m3 bytes (row-major, 16-byte aligned rows).
+ * d_scaleA: nb fp32 row scales (SCALED only).  Outputs (nb, k) row-major:
+ * d_vals fp32 descending, d_locs int32 1-based global column ids.
+ * Ties are ordered by ascending column. */
+int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A,
+                        const float *d_scaleA, int nb, float *d_vals,
+                        int32_t *d_locs, r2m_stream_t stream);
+
+/* ------------------------------------------------------------ host FASTA */
+
+typedef struct r2m_reads r2m_reads;
+
+/* Replaces fasta_reads (RotorMap/fasta/reader.jl:321-350) with _LUT3/_emit3!
+ * semantics (reader.jl:21-28,120-198): every record's sequence is packed to
+ * forward 2-bit words, trimmed to its first k bases; records with fewer
+ * than k bases are skipped; headers are kept verbatim with the '>'.
+ * Records are returned in file order.  `data` need not be NUL-terminated. */
+int r2m_fasta_reads(const char *data, size_t len, int k, int nthreads,
+                    r2m_reads **out);
+int64_t r2m_reads_count(const r2m_reads *r);
+/* r2m_reads_count(r) * cld(k,16) words, fragment-major. */
+const uint32_t *r2m_reads_words(const r2m_reads *r);
+/* Header i (not NUL-terminated); its byte length in *len. */
+const char *r2m_reads_header(const r2m_reads *r, int64_t i, size_t *len);
+void r2m_reads_free(r2m_reads *r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R2M_H */

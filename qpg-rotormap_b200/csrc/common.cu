@@ -1,0 +1,101 @@
+// common.cu -- host side of the C ABI plumbing: thread-local last error,
+// cached device properties and the per-device error word that bounded
+// device-side waits report through.
+#include <mutex>
+#include <string>
+
+#include "common.cuh"
+
+namespace r2m {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" +
+                 cudaGetErrorString(e) + ")";
+  return R2M_ECUDA;
+}
+
+static const int kMaxDev = 64;
+static std::mutex g_mu;
+static int g_sm[kMaxDev];
+static uint32_t *g_errword[kMaxDev];
+
+int sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 148;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_sm[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    g_sm[dev] = n;
+  }
+  return g_sm[dev];
+}
+
+int device_error_word(uint32_t **out) {
+  int dev = 0;
+  R2M_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDev) return fail(R2M_ESTATE, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_errword[dev] == nullptr) {
+    uint32_t *p = nullptr;
+    R2M_CUDA(cudaMalloc(&p, sizeof(uint32_t)));
+    R2M_CUDA(cudaMemset(p, 0, sizeof(uint32_t)));
+    R2M_CUDA(cudaDeviceSynchronize());
+    g_errword[dev] = p;
+  }
+  *out = g_errword[dev];
+  return R2M_OK;
+}
+
+int check_device_error(cudaStream_t stream, const char *what) {
+  uint32_t *w = nullptr;
+  int rc = device_error_word(&w);
+  if (rc) return rc;
+  uint32_t h = 0;
+  R2M_CUDA(cudaMemcpyAsync(&h, w, sizeof(h), cudaMemcpyDeviceToHost, stream));
+  R2M_CUDA(cudaStreamSynchronize(stream));
+  if (h != 0) {
+    R2M_CUDA(cudaMemsetAsync(w, 0, sizeof(uint32_t), stream));
+    R2M_CUDA(cudaStreamSynchronize(stream));
+    return fail(R2M_ETIMEOUT, std::string(what) + ": a bounded device wait gave up (code " +
+                                  std::to_string(h) + "); the kernel aborted its work");
+  }
+  return R2M_OK;
+}
+
+}  // namespace r2m
+
+extern "C" {
+
+const char *r2m_last_error(void) { return r2m::g_last_error.c_str(); }
+
+int r2m_version(void) { return 10000; }
+
+int r2m_check_device_error(r2m_stream_t stream) {
+  return r2m::check_device_error(r2m::as_stream(stream), "r2m_check_device_error");
+}
+
+int r2m_device_check(void) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return r2m::cuda_fail(e, "cudaGetDevice");
+  int major = 0;
+  e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (e != cudaSuccess) return r2m::cuda_fail(e, "cudaDeviceGetAttribute");
+  if (major != 10)
+    return r2m::fail(R2M_ESTATE, "librotormap_b200 needs an sm_100 (B200) device, found cc " +
+                                     std::to_string(major) + ".x");
+  return R2M_OK;
+}
+
+}  // extern "C"

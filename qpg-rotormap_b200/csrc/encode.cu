@@ -1,0 +1,650 @@
+// encode.cu -- the fused rope encoder (reads and index windows), the
+// reverse-complement word kernel and the e4m3 quantisers.
+//
+// Encoder semantics follow the reference kernel kernel_rope_frag_real
+// (RotorMap/encode/kernel.jl:86-290) and its fp64 twin _ref_rope_frag
+// (RotorMap/encode/reference.jl:37-93):
+//   * window p (0-based, p < nw = k-s+1) reads the little-endian 2s-bit field
+//     of bases [p, p+s): smer = (stream >> 2p) & (4^s-1);
+//   * lower = smer & (4^c-1), upper = smer >> 2c,
+//     csmer = lower ^ ((upper * 0x9E3779B1) & (4^c-1));
+//   * bin = csmer*m + idm gets the phasor exp(+i*theta_idm*p) with
+//     theta_idm = f32(factor) * f32(2*pi/k), factor = 1 (m = 1) else
+//     2*idm/(m-1)+1 (idm 0-based);
+//   * the bins of csmer 2*sum_{i<c} 4^i ("GG..G") are zeroed;
+//   * normalize modes 0..3 as the reference; the real row is the split
+//     [Re(bin 0..D-1); Im(bin 0..D-1)], D = m*4^c.
+//
+// B200 design: one warp per fragment (the reference spends one 512-thread
+// block per 150-base read with 143 active threads).  The phasor of every
+// (idm, p) is computed once per block into shared memory with the exact fp32
+// recipe of the reference thread that owns window p (direct cos/sin at the
+// thread's first window, then the fp32 complex recurrence), so the values
+// are the reference's.  Histogram sums are deterministic: windows are added
+// to their bins in increasing p (warp match_any groups equal bins inside a
+// 32-window batch; the group's leader adds them in lane order).  The output
+// conversion (fp32 / fp16 / e4m3 / scaled e4m3) is fused into the final pass.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace r2m {
+
+struct EncParams {
+  int k, s, m, c, normalize;
+  int W;      // words per fragment = cld(k,16)
+  int nw;     // windows = k-s+1
+  int nbin;   // complex bins D = m*4^c
+  int rdim;   // 2*nbin
+  int Wc;     // the reference thread chunk: cld(nw,512), made odd
+  uint32_t bmask, cbmask, csmerG;
+  float theta[8];  // per idm, fp32
+  int table_in_smem;
+  int hist_floats;  // per-warp histogram floats (2*nbin, rounded to 4)
+  int cs_u16;       // per-warp csmer slots (nw rounded up to 8)
+  int words_u32;    // per-warp staged words (W + 2, rounded up to 4)
+};
+
+static int make_params(EncParams &P, int k, int s, int m, int c, int normalize) {
+  R2M_REQUIRE(s >= 1 && s <= 16, "s must be in 1..16 (the s-mer lives in a 32-bit funnel window)");
+  R2M_REQUIRE(c >= 1 && c <= s, "c must be in 1..s");
+  R2M_REQUIRE(m >= 1 && m <= 8, "m must be in 1..8");
+  R2M_REQUIRE(k >= s, "k must be >= s (no s-mer windows otherwise)");
+  R2M_REQUIRE(k <= (1 << 22), "k too large");
+  R2M_REQUIRE(normalize >= 0 && normalize <= 3, "normalize must be 0..3");
+  R2M_REQUIRE((long long)m << (2 * c) <= 16384, "m*4^c too large for the shared-memory histogram");
+  P.k = k; P.s = s; P.m = m; P.c = c; P.normalize = normalize;
+  P.W = (k + 15) / 16;
+  P.nw = k - s + 1;
+  P.nbin = m << (2 * c);
+  P.rdim = 2 * P.nbin;
+  int wc = (P.nw + 511) / 512;
+  if ((wc & 1) == 0) wc += 1;
+  P.Wc = wc;
+  P.bmask = (s == 16) ? 0xFFFFFFFFu : ((1u << (2 * s)) - 1u);
+  P.cbmask = (c == 16) ? 0xFFFFFFFFu : ((1u << (2 * c)) - 1u);
+  uint32_t allones = 0;
+  for (int i = 0; i < c; ++i) allones += 1u << (2 * i);
+  P.csmerG = 2u * allones;  // 0-based index of the reference's 2*allones+1
+  float base = (float)(2.0 * M_PI / (double)k);
+  for (int i = 0; i < 8; ++i) {
+    float f = (m == 1) ? 1.0f : (float)(2.0 * (double)i / (double)(m - 1) + 1.0);
+    P.theta[i] = f * base;
+  }
+  P.hist_floats = (P.rdim + 3) & ~3;
+  P.cs_u16 = (P.nw + 7) & ~7;
+  P.words_u32 = (P.W + 2 + 3) & ~3;
+  return R2M_OK;
+}
+
+// Exact reference phasor of window p for copy idm (see file header).
+__device__ __forceinline__ float2 ref_phasor(const EncParams &P, int idm, int p) {
+  float th = P.theta[idm];
+  int p0 = (p / P.Wc) * P.Wc;
+  float a = th * (float)p0;
+  float re = cosf(a), im = sinf(a);
+  if (p != p0) {
+    float xr = cosf(th), xi = sinf(th);
+    for (int q = p0; q < p; ++q) {
+      float nr = __fsub_rn(__fmul_rn(re, xr), __fmul_rn(im, xi));
+      float ni = __fadd_rn(__fmul_rn(re, xi), __fmul_rn(im, xr));
+      re = nr;
+      im = ni;
+    }
+  }
+  return make_float2(re, im);
+}
+
+// Global table (used when the per-block shared copy does not fit):
+// one thread per (idm, reference chunk) walks the chunk's recurrence.
+__global__ void k_phasor_table(EncParams P, float2 *table) {
+  int nchunk = (P.nw + P.Wc - 1) / P.Wc;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nchunk * P.m) return;
+  int idm = t / nchunk, ch = t % nchunk;
+  int p0 = ch * P.Wc, p1 = min(p0 + P.Wc, P.nw);
+  float th = P.theta[idm];
+  float a = th * (float)p0;
+  float re = cosf(a), im = sinf(a);
+  float xr = cosf(th), xi = sinf(th);
+  for (int p = p0; p < p1; ++p) {
+    table[(size_t)idm * P.nw + p] = make_float2(re, im);
+    float nr = __fsub_rn(__fmul_rn(re, xr), __fmul_rn(im, xi));
+    float ni = __fadd_rn(__fmul_rn(re, xi), __fmul_rn(im, xr));
+    re = nr;
+    im = ni;
+  }
+}
+
+template <int OUT>
+struct OutT;
+template <>
+struct OutT<R2M_OUT_F32> { static constexpr int bytes = 4; };
+template <>
+struct OutT<R2M_OUT_F16> { static constexpr int bytes = 2; };
+template <>
+struct OutT<R2M_OUT_E4M3> { static constexpr int bytes = 1; };
+template <>
+struct OutT<R2M_OUT_E4M3_SCALED> { static constexpr int bytes = 1; };
+
+template <int OUT>
+__device__ __forceinline__ void store16(void *row, int i0, const float (&v)[16]) {
+  if constexpr (OUT == R2M_OUT_F32) {
+    float4 *d = reinterpret_cast<float4 *>(reinterpret_cast<float *>(row) + i0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  } else if constexpr (OUT == R2M_OUT_F16) {
+    uint32_t h[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      __half2 t = __floats2half2_rn(v[2 * q], v[2 * q + 1]);
+      h[q] = *reinterpret_cast<uint32_t *>(&t);
+    }
+    uint4 *d = reinterpret_cast<uint4 *>(reinterpret_cast<__half *>(row) + i0);
+    d[0] = make_uint4(h[0], h[1], h[2], h[3]);
+    d[1] = make_uint4(h[4], h[5], h[6], h[7]);
+  } else {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t lo = f32x2_to_e4m3x2(v[4 * q], v[4 * q + 1]);
+      uint32_t hi = f32x2_to_e4m3x2(v[4 * q + 2], v[4 * q + 3]);
+      w[q] = lo | (hi << 16);
+    }
+    *reinterpret_cast<uint4 *>(reinterpret_cast<uint8_t *>(row) + i0) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+template <int OUT>
+__device__ __forceinline__ void store1(void *row, int i, float v) {
+  if constexpr (OUT == R2M_OUT_F32) {
+    reinterpret_cast<float *>(row)[i] = v;
+  } else if constexpr (OUT == R2M_OUT_F16) {
+    reinterpret_cast<__half *>(row)[i] = __float2half_rn(v);
+  } else {
+    reinterpret_cast<uint8_t *>(row)[i] = f32_to_e4m3(v);
+  }
+}
+
+// Value of output element i (split layout) before the storage conversion.
+// E4M3 parity mode rounds through fp16 first, like the reference's fp16
+// stream followed by f32_to_f8 of the widened value.
+template <int OUT>
+__device__ __forceinline__ float out_value(const EncParams &P, const float *hist,
+                                           const float *nrmv, int i, float scale) {
+  int bin = (i < P.nbin) ? i : i - P.nbin;
+  int part = (i < P.nbin) ? 0 : 1;
+  float nrm = nrmv[P.normalize == 0 ? 0 : (bin % P.m)];
+  float x = hist[2 * bin + part] / nrm;
+  if constexpr (OUT == R2M_OUT_E4M3) x = __half2float(__float2half_rn(x));
+  if constexpr (OUT == R2M_OUT_E4M3_SCALED) x = x * scale;
+  return x;
+}
+
+// Encode the fragment whose words are staged in `words` (W words + a zero
+// guard word) with one warp; write row `row` (rdim elements of OUT), the m
+// norms and (scaled e4m3) the row scale.
+template <int OUT>
+__device__ void encode_fragment(const EncParams &P, const float2 *table, float *hist,
+                                uint16_t *cs, const uint32_t *words, float *nrmv, void *row,
+                                float *norms_out, float *scale_out) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+  // zero the histogram
+  for (int i = lane * 4; i < P.hist_floats; i += 128)
+    *reinterpret_cast<float4 *>(hist + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+  // scrambled c-mer of every window
+  for (int p = lane; p < P.nw; p += 32) {
+    int wo = p >> 4;
+    uint32_t sh = (uint32_t)(p & 15) << 1;
+    uint32_t w0 = words[wo], w1 = words[wo + 1];
+    uint32_t v = sh == 0 ? w0 : ((w0 >> sh) | (w1 << (32u - sh)));
+    uint32_t smer = v & P.bmask;
+    uint32_t lower = smer & P.cbmask;
+    uint32_t upper = (2 * P.c >= 32) ? 0u : (smer >> (2 * P.c));
+    uint32_t key = (upper * 0x9E3779B1u) & P.cbmask;
+    cs[p] = (uint16_t)(lower ^ key);
+  }
+  __syncwarp();
+  // accumulate phasors in increasing window order (deterministic)
+  for (int b0 = 0; b0 < P.nw; b0 += 32) {
+    int p = b0 + lane;
+    bool act = p < P.nw;
+    unsigned amask = __ballot_sync(FULL, act);
+    if (act) {
+      uint32_t cbin = cs[p];
+      unsigned grp = __match_any_sync(amask, cbin);
+      if (lane == __ffs(grp) - 1) {
+        for (int idm = 0; idm < P.m; ++idm) {
+          float *h = hist + 2 * (cbin * P.m + idm);
+          float re = h[0], im = h[1];
+          const float2 *tb = table + (size_t)idm * P.nw + b0;
+          unsigned g = grp;
+          while (g) {
+            int j = __ffs(g) - 1;
+            g &= g - 1;
+            float2 ph = tb[j];
+            re += ph.x;
+            im += ph.y;
+          }
+          h[0] = re;
+          h[1] = im;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // zero the G-homopolymer bins
+  if (lane < P.m) {
+    float *h = hist + 2 * (P.csmerG * P.m + lane);
+    h[0] = 0.f;
+    h[1] = 0.f;
+  }
+  __syncwarp();
+  // modes 2/3 reshape every bin first (fp64 arithmetic, fp32 storage)
+  if (P.normalize >= 2) {
+    for (int b = lane; b < P.nbin; b += 32) {
+      float re = hist[2 * b], im = hist[2 * b + 1];
+      double a = (double)hypotf(re, im);
+      double d = (P.normalize == 2) ? (a + 2.220446049250313e-16) : sqrt(a + 2.220446049250313e-16);
+      hist[2 * b] = (float)((double)re / d);
+      hist[2 * b + 1] = (float)((double)im / d);
+    }
+    __syncwarp();
+  }
+  // per-copy sums of squares
+  float part[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) part[t] = 0.f;
+  for (int b = lane; b < P.nbin; b += 32) {
+    float re = hist[2 * b], im = hist[2 * b + 1];
+    float e = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
+    int t = b % P.m;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (q == t) part[q] += e;
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part[q] += __shfl_xor_sync(FULL, part[q], o);
+  }
+  if (lane == 0) {
+    if (P.normalize == 0) {
+      float acc = part[0];
+      for (int q = 1; q < P.m; ++q) acc += part[q];
+      float nrm = (float)((double)sqrtf(acc) + 1e-16);
+      nrmv[0] = nrm;
+      norms_out[0] = nrm;
+      for (int q = 1; q < P.m; ++q) norms_out[q] = part[q];
+    } else {
+      for (int q = 0; q < P.m; ++q) {
+        float nrm;
+        if (P.normalize == 1) nrm = sqrtf(part[q]) + 1e-7f;
+        else nrm = (float)((double)sqrtf(part[q]) + 2.220446049250313e-16);
+        nrmv[q] = nrm;
+        norms_out[q] = nrm;
+      }
+    }
+  }
+  __syncwarp();
+  // output pass (amax first for the scaled form)
+  float scale = 1.0f;
+  if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
+    float amax = 0.f;
+    for (int i = lane; i < P.rdim; i += 32)
+      amax = fmaxf(amax, fabsf(out_value<R2M_OUT_F32>(P, hist, nrmv, i, 1.0f)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(FULL, amax, o));
+    scale = amax > 0.f ? 448.0f / amax : 1.0f;
+    if (lane == 0) *scale_out = amax > 0.f ? amax / 448.0f : 0.0f;
+  }
+  const bool vec = (P.rdim % 16) == 0;
+  if (vec) {
+    for (int i0 = lane * 16; i0 < P.rdim; i0 += 512) {
+      float v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = out_value<OUT>(P, hist, nrmv, i0 + j, scale);
+      store16<OUT>(row, i0, v);
+    }
+  } else {
+    for (int i = lane; i < P.rdim; i += 32) store1<OUT>(row, i, out_value<OUT>(P, hist, nrmv, i, scale));
+  }
+  __syncwarp();
+}
+
+// Per-warp shared-memory carve-up.
+struct WarpSmem {
+  float *hist;
+  uint16_t *cs;
+  uint32_t *words;
+  uint32_t *words2;  // second word buffer (reverse complement)
+  float *nrmv;
+};
+
+__device__ __forceinline__ size_t warp_smem_bytes(const EncParams &P) {
+  return (size_t)P.hist_floats * 4 + (size_t)P.cs_u16 * 2 + (size_t)P.words_u32 * 4 * 2 + 32;
+}
+
+__device__ __forceinline__ WarpSmem carve(const EncParams &P, unsigned char *base, int warp) {
+  size_t per = warp_smem_bytes(P);
+  unsigned char *p = base + per * warp;
+  WarpSmem w;
+  w.hist = reinterpret_cast<float *>(p);
+  p += (size_t)P.hist_floats * 4;
+  w.words = reinterpret_cast<uint32_t *>(p);
+  p += (size_t)P.words_u32 * 4;
+  w.words2 = reinterpret_cast<uint32_t *>(p);
+  p += (size_t)P.words_u32 * 4;
+  w.nrmv = reinterpret_cast<float *>(p);
+  p += 32;
+  w.cs = reinterpret_cast<uint16_t *>(p);
+  return w;
+}
+
+// Block prologue: the phasor table in shared memory (or the global copy).
+__device__ __forceinline__ const float2 *block_table(const EncParams &P, unsigned char *smem,
+                                                     const float2 *gtable) {
+  if (!P.table_in_smem) return gtable;
+  float2 *t = reinterpret_cast<float2 *>(smem);
+  int total = P.m * P.nw;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    int idm = i / P.nw, p = i % P.nw;
+    t[i] = ref_phasor(P, idm, p);
+  }
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ size_t table_bytes(const EncParams &P) {
+  return P.table_in_smem ? (((size_t)P.m * P.nw * 8 + 15) & ~(size_t)15) : 0;
+}
+
+template <int OUT>
+__global__ void __launch_bounds__(256) k_encode_frags(EncParams P, const uint32_t *__restrict__ dnas,
+                                                      int64_t n, void *dest, float *norms,
+                                                      float *scales, const float2 *gtable) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const float2 *table = block_table(P, smem, gtable);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem ws = carve(P, smem + table_bytes(P), warp);
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const size_t rowbytes = (size_t)P.rdim * OutT<OUT>::bytes;
+  for (int64_t f = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; f < n; f += nwarps) {
+    const uint32_t *src = dnas + f * P.W;
+    for (int i = lane; i < P.W; i += 32) ws.words[i] = __ldg(src + i);
+    if (lane == 0) ws.words[P.W] = 0u;
+    __syncwarp();
+    encode_fragment<OUT>(P, table, ws.hist, ws.cs, ws.words, ws.nrmv,
+                         reinterpret_cast<unsigned char *>(dest) + rowbytes * f,
+                         norms + f * P.m, scales ? scales + f : nullptr);
+  }
+}
+
+// Index windows: forward window from the packed genome, then its reverse
+// complement, into the reference's per-batch [fwd block | rc block] columns.
+template <int OUT>
+__global__ void __launch_bounds__(256) k_encode_ref(EncParams P, const uint32_t *__restrict__ genome,
+                                                    const int64_t *__restrict__ win_pos,
+                                                    int64_t nwin, int64_t batch, void *dest,
+                                                    float *norms, float *scales,
+                                                    const float2 *gtable) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const float2 *table = block_table(P, smem, gtable);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem ws = carve(P, smem + table_bytes(P), warp);
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const size_t rowbytes = (size_t)P.rdim * OutT<OUT>::bytes;
+  const int r = P.k & 15;
+  const uint32_t tailmask = r == 0 ? 0xFFFFFFFFu : ((1u << (2 * r)) - 1u);
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; i < nwin; i += nwarps) {
+    const int64_t pos = __ldg(win_pos + i);
+    const int64_t q = pos >> 4;
+    const uint32_t sh = (uint32_t)(pos & 15) << 1;
+    for (int j = lane; j < P.W; j += 32) {
+      uint32_t a = __ldg(genome + q + j), b = __ldg(genome + q + j + 1);
+      uint32_t v = sh == 0 ? a : ((a >> sh) | (b << (32u - sh)));
+      if (j == P.W - 1) v &= tailmask;
+      ws.words[j] = v;
+    }
+    if (lane == 0) ws.words[P.W] = 0u;
+    __syncwarp();
+    // reverse complement: rc base j = 3 - fwd base (k-1-j)
+    for (int j = lane; j < P.W; j += 32) {
+      uint32_t w = 0;
+      for (int b = 0; b < 16; ++b) {
+        int t = 16 * j + b;
+        if (t < P.k) {
+          int src = P.k - 1 - t;
+          uint32_t code = (ws.words[src >> 4] >> (2 * (src & 15))) & 3u;
+          w |= (3u - code) << (2 * b);
+        }
+      }
+      ws.words2[j] = w;
+    }
+    if (lane == 0) ws.words2[P.W] = 0u;
+    __syncwarp();
+    const int64_t b = i / batch, off = i - b * batch;
+    const int64_t nb = min(batch, nwin - b * batch);
+    const int64_t colf = 2 * b * batch + off, colr = colf + nb;
+    encode_fragment<OUT>(P, table, ws.hist, ws.cs, ws.words, ws.nrmv,
+                         reinterpret_cast<unsigned char *>(dest) + rowbytes * colf,
+                         norms + colf * P.m, scales ? scales + colf : nullptr);
+    encode_fragment<OUT>(P, table, ws.hist, ws.cs, ws.words2, ws.nrmv,
+                         reinterpret_cast<unsigned char *>(dest) + rowbytes * colr,
+                         norms + colr * P.m, scales ? scales + colr : nullptr);
+  }
+}
+
+__device__ __forceinline__ uint32_t lanerev32(uint32_t x) {
+  x = ((x & 0x33333333u) << 2) | ((x >> 2) & 0x33333333u);
+  x = ((x & 0x0F0F0F0Fu) << 4) | ((x >> 4) & 0x0F0F0F0Fu);
+  x = ((x & 0x00FF00FFu) << 8) | ((x >> 8) & 0x00FF00FFu);
+  return (x << 16) | (x >> 16);
+}
+
+// One thread per output word: complement, left-align the k bases to the end
+// of the W-word stream, then reverse word order and the sixteen 2-bit lanes.
+__global__ void k_revcomp(uint32_t *drc, const uint32_t *dnas, int W, int64_t n, uint32_t shbits) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)W * n) return;
+  int64_t f = g / W;
+  int p = (int)(g - f * W);
+  int i = W - 1 - p;
+  const uint32_t *src = dnas + f * W;
+  uint32_t x = ~src[i];
+  uint32_t v = x;
+  if (shbits != 0) v = (x << shbits) | (i > 0 ? ((~src[i - 1]) >> (32u - shbits)) : 0u);
+  drc[g] = lanerev32(v);
+}
+
+__global__ void k_f32_to_e4m3(uint8_t *dst, const float *src, int64_t count) {
+  int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
+  for (; i < count; i += stride) {
+    if (i + 4 <= count && ((reinterpret_cast<uintptr_t>(src + i) & 15) == 0)) {
+      float4 v = *reinterpret_cast<const float4 *>(src + i);
+      uint32_t lo = f32x2_to_e4m3x2(v.x, v.y), hi = f32x2_to_e4m3x2(v.z, v.w);
+      uint32_t w = lo | (hi << 16);
+      dst[i] = w & 0xFF; dst[i + 1] = (w >> 8) & 0xFF; dst[i + 2] = (w >> 16) & 0xFF; dst[i + 3] = w >> 24;
+    } else {
+      for (int64_t j = i; j < i + 4 && j < count; ++j) dst[j] = f32_to_e4m3(src[j]);
+    }
+  }
+}
+
+__global__ void k_f16_to_e4m3(uint8_t *dst, const __half *src, int64_t count) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+    dst[i] = f32_to_e4m3(__half2float(src[i]));
+}
+
+// ------------------------------------------------------------------ host
+
+static size_t warp_bytes_host(const EncParams &P) {
+  return (size_t)P.hist_floats * 4 + (size_t)P.cs_u16 * 2 + (size_t)P.words_u32 * 4 * 2 + 32;
+}
+
+template <int OUT, typename KernelFn>
+static int plan_launch(EncParams &P, KernelFn kern, int64_t nwork, int *grid, int *block,
+                       size_t *smem, float2 **gtable, cudaStream_t st) {
+  const size_t kSmemCap = 200 * 1024;
+  size_t tb = ((size_t)P.m * P.nw * 8 + 15) & ~(size_t)15;
+  size_t wb = warp_bytes_host(P);
+  P.table_in_smem = (tb + wb * 2 <= 100 * 1024) ? 1 : 0;
+  size_t fixed = P.table_in_smem ? tb : 0;
+  int wpb = 8;
+  while (wpb > 1 && fixed + wb * wpb > kSmemCap) wpb >>= 1;
+  if (fixed + wb * wpb > kSmemCap) return fail(R2M_EINVAL, "encoder shared memory does not fit (k or m*4^c too large)");
+  *block = 32 * wpb;
+  *smem = fixed + wb * wpb;
+  R2M_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  int per_sm = 0;
+  R2M_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, *block, *smem));
+  if (per_sm < 1) per_sm = 1;
+  int64_t want = (nwork + wpb - 1) / wpb;
+  int64_t cap = (int64_t)sm_count() * per_sm;
+  *grid = (int)(want < cap ? want : cap);
+  if (*grid < 1) *grid = 1;
+  *gtable = nullptr;
+  if (!P.table_in_smem) {
+    float2 *t = nullptr;
+    R2M_CUDA(cudaMallocAsync(&t, (size_t)P.m * P.nw * sizeof(float2), st));
+    int nchunk = (P.nw + P.Wc - 1) / P.Wc;
+    int tot = nchunk * P.m;
+    k_phasor_table<<<(tot + 127) / 128, 128, 0, st>>>(P, t);
+    R2M_CUDA(cudaGetLastError());
+    *gtable = t;
+  }
+  return R2M_OK;
+}
+
+template <int OUT>
+static int launch_frags(EncParams P, void *dest, float *norms, float *scales, const uint32_t *dnas,
+                        int64_t n, cudaStream_t st) {
+  int grid, block;
+  size_t smem;
+  float2 *gt = nullptr;
+  int rc = plan_launch<OUT>(P, k_encode_frags<OUT>, n, &grid, &block, &smem, &gt, st);
+  if (rc) return rc;
+  k_encode_frags<OUT><<<grid, block, smem, st>>>(P, dnas, n, dest, norms, scales, gt);
+  cudaError_t e = cudaGetLastError();
+  if (gt) cudaFreeAsync(gt, st);
+  if (e != cudaSuccess) return cuda_fail(e, "k_encode_frags launch");
+  return R2M_OK;
+}
+
+template <int OUT>
+static int launch_ref(EncParams P, void *dest, float *norms, float *scales, const uint32_t *genome,
+                      const int64_t *pos, int64_t nwin, int64_t batch, cudaStream_t st) {
+  int grid, block;
+  size_t smem;
+  float2 *gt = nullptr;
+  int rc = plan_launch<OUT>(P, k_encode_ref<OUT>, nwin, &grid, &block, &smem, &gt, st);
+  if (rc) return rc;
+  k_encode_ref<OUT><<<grid, block, smem, st>>>(P, genome, pos, nwin, batch, dest, norms, scales, gt);
+  cudaError_t e = cudaGetLastError();
+  if (gt) cudaFreeAsync(gt, st);
+  if (e != cudaSuccess) return cuda_fail(e, "k_encode_ref launch");
+  return R2M_OK;
+}
+
+static int check_align(const void *p, size_t a, const char *what) {
+  if ((reinterpret_cast<uintptr_t>(p) % a) != 0)
+    return fail(R2M_EINVAL, std::string(what) + " must be " + std::to_string(a) + "-byte aligned");
+  return R2M_OK;
+}
+
+}  // namespace r2m
+
+using namespace r2m;
+
+extern "C" int r2m_encode_frag_real_batch(void *dest, int out_kind, float *dest_norms,
+                                          float *dest_scales, const uint32_t *dnas, int64_t n,
+                                          int k, int s, int m, int c, int normalize,
+                                          r2m_stream_t stream) {
+  EncParams P;
+  int rc = make_params(P, k, s, m, c, normalize);
+  if (rc) return rc;
+  R2M_REQUIRE(n >= 0, "n must be >= 0");
+  if (n == 0) return R2M_OK;
+  R2M_REQUIRE(dest && dest_norms && dnas, "null pointer");
+  R2M_REQUIRE(out_kind >= R2M_OUT_F32 && out_kind <= R2M_OUT_E4M3_SCALED, "bad out_kind");
+  R2M_REQUIRE(out_kind != R2M_OUT_E4M3_SCALED || dest_scales, "scaled e4m3 needs dest_scales");
+  if ((rc = check_align(dest, 16, "dest"))) return rc;
+  cudaStream_t st = as_stream(stream);
+  switch (out_kind) {
+    case R2M_OUT_F32: return launch_frags<R2M_OUT_F32>(P, dest, dest_norms, nullptr, dnas, n, st);
+    case R2M_OUT_F16: return launch_frags<R2M_OUT_F16>(P, dest, dest_norms, nullptr, dnas, n, st);
+    case R2M_OUT_E4M3: return launch_frags<R2M_OUT_E4M3>(P, dest, dest_norms, nullptr, dnas, n, st);
+    default: return launch_frags<R2M_OUT_E4M3_SCALED>(P, dest, dest_norms, dest_scales, dnas, n, st);
+  }
+}
+
+extern "C" int r2m_encode_ref_windows(void *dest, int out_kind, float *dest_norms,
+                                      float *dest_scales, const uint32_t *genome,
+                                      const int64_t *win_pos, int64_t nwin, int64_t batch_size,
+                                      int k, int s, int m, int c, int normalize,
+                                      r2m_stream_t stream) {
+  EncParams P;
+  int rc = make_params(P, k, s, m, c, normalize);
+  if (rc) return rc;
+  R2M_REQUIRE(nwin >= 0, "nwin must be >= 0");
+  R2M_REQUIRE(batch_size >= 1, "batch_size must be >= 1");
+  if (nwin == 0) return R2M_OK;
+  R2M_REQUIRE(dest && dest_norms && genome && win_pos, "null pointer");
+  R2M_REQUIRE(out_kind >= R2M_OUT_F32 && out_kind <= R2M_OUT_E4M3_SCALED, "bad out_kind");
+  R2M_REQUIRE(out_kind != R2M_OUT_E4M3_SCALED || dest_scales, "scaled e4m3 needs dest_scales");
+  if ((rc = check_align(dest, 16, "dest"))) return rc;
+  cudaStream_t st = as_stream(stream);
+  switch (out_kind) {
+    case R2M_OUT_F32:
+      return launch_ref<R2M_OUT_F32>(P, dest, dest_norms, nullptr, genome, win_pos, nwin, batch_size, st);
+    case R2M_OUT_F16:
+      return launch_ref<R2M_OUT_F16>(P, dest, dest_norms, nullptr, genome, win_pos, nwin, batch_size, st);
+    case R2M_OUT_E4M3:
+      return launch_ref<R2M_OUT_E4M3>(P, dest, dest_norms, nullptr, genome, win_pos, nwin, batch_size, st);
+    default:
+      return launch_ref<R2M_OUT_E4M3_SCALED>(P, dest, dest_norms, dest_scales, genome, win_pos, nwin,
+                                             batch_size, st);
+  }
+}
+
+extern "C" int r2m_revcomp_frag_words(uint32_t *drc, const uint32_t *dnas, int k, int64_t n,
+                                      r2m_stream_t stream) {
+  R2M_REQUIRE(k >= 1, "k must be >= 1");
+  R2M_REQUIRE(n >= 0, "n must be >= 0");
+  if (n == 0) return R2M_OK;
+  R2M_REQUIRE(drc && dnas, "null pointer");
+  int W = (k + 15) / 16;
+  uint32_t sh = (uint32_t)(32 * W - 2 * k);
+  int64_t total = (int64_t)W * n;
+  int64_t blocks = (total + 255) / 256;
+  k_revcomp<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(drc, dnas, W, n, sh);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
+
+extern "C" int r2m_f32_to_e4m3(uint8_t *dst, const float *src, int64_t count, r2m_stream_t stream) {
+  R2M_REQUIRE(count >= 0, "count must be >= 0");
+  if (count == 0) return R2M_OK;
+  R2M_REQUIRE(dst && src, "null pointer");
+  int64_t blocks = (count / 4 + 255) / 256 + 1;
+  if (blocks > 65535) blocks = 65535;
+  k_f32_to_e4m3<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(dst, src, count);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
+
+extern "C" int r2m_f16_to_e4m3(uint8_t *dst, const uint16_t *src, int64_t count, r2m_stream_t stream) {
+  R2M_REQUIRE(count >= 0, "count must be >= 0");
+  if (count == 0) return R2M_OK;
+  R2M_REQUIRE(dst && src, "null pointer");
+  int64_t blocks = (count + 255) / 256;
+  if (blocks > 65535) blocks = 65535;
+  k_f16_to_e4m3<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(dst, reinterpret_cast<const __half *>(src),
+                                                                  count);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}

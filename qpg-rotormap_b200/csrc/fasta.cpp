@@ -1,0 +1,176 @@
+// fasta.cpp -- host FASTA reader: records -> forward 2-bit words, trimmed
+// to the first k bases (records shorter than k are skipped).
+//
+// Semantics of fasta_reads / _next_rec3 / _collect3! / _emit3!
+// (RotorMap/fasta/reader.jl:21-28,61-75,120-198,204-311):
+//   * a record starts at a '>' that is the first byte of the input or
+//     follows '\n' or '\r'; bytes before the first record are ignored;
+//   * the header is the '>' line up to (excluding) the first '\n', one
+//     trailing '\r' removed; a header line that is not closed by '\n' before
+//     the next record start (or the end of input) ends the parse;
+//   * every sequence byte except '\n'/'\r' is a base: A/C/G/T (either case)
+//     -> 0/1/2/3, anything else -> 2 (G);
+//   * base j sits in word j>>4 at bits 2*(j&15); the tail is zero-padded.
+// Records come back in file order.  Large inputs are split at record
+// boundaries and parsed by several threads; the result does not depend on
+// the thread count.
+#include <string.h>
+
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "r2m.h"
+
+namespace r2m {
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+}  // namespace r2m
+
+struct r2m_reads {
+  int k = 0, W = 0;
+  std::vector<uint32_t> words;
+  std::vector<size_t> hoff;  // header offsets into `heads` (n+1 entries)
+  std::string heads;
+};
+
+namespace {
+
+struct Lut {
+  uint8_t code[256];
+  Lut() {
+    for (int i = 0; i < 256; ++i) code[i] = 2;
+    code[(int)'A'] = 0; code[(int)'C'] = 1; code[(int)'G'] = 2; code[(int)'T'] = 3;
+    code[(int)'a'] = 0; code[(int)'c'] = 1; code[(int)'g'] = 2; code[(int)'t'] = 3;
+  }
+};
+const Lut kLut;
+
+inline bool is_rec_start(const char *d, size_t i) {
+  return d[i] == '>' && (i == 0 || d[i - 1] == '\n' || d[i - 1] == '\r');
+}
+
+// first record start in [from, hi), or hi
+size_t next_rec(const char *d, size_t from, size_t hi) {
+  size_t p = from;
+  while (p < hi) {
+    const void *q = memchr(d + p, '>', hi - p);
+    if (!q) return hi;
+    size_t t = (size_t)((const char *)q - d);
+    if (is_rec_start(d, t)) return t;
+    p = t + 1;
+  }
+  return hi;
+}
+
+struct Part {
+  std::vector<uint32_t> words;
+  std::vector<size_t> hlen;
+  std::string heads;
+  bool stop = false;  // an unterminated header line ended the parse here
+};
+
+// Parse the records whose starts lie in [lo, hi) (lo is a record start or
+// hi); sequences may run to `end` (the record's own next start).
+void parse_range(const char *d, size_t n, size_t lo, size_t hi, int k, Part &out) {
+  const int W = (k + 15) / 16;
+  std::vector<uint32_t> w(W);
+  size_t s = lo;
+  while (s < hi) {
+    size_t e = next_rec(d, s + 1, n);
+    size_t h = s;
+    while (h < e && d[h] != '\n') ++h;
+    if (h == e) {  // header not closed before the next record / EOF
+      out.stop = true;
+      return;
+    }
+    size_t hend = h;  // exclusive
+    if (hend > s && d[hend - 1] == '\r') --hend;
+    // collect the first k bases of [h+1, e)
+    std::fill(w.begin(), w.end(), 0u);
+    int bases = 0;
+    for (size_t p = h + 1; p < e && bases < k; ++p) {
+      char c = d[p];
+      if (c == '\n' || c == '\r') continue;
+      w[bases >> 4] |= (uint32_t)kLut.code[(uint8_t)c] << (2 * (bases & 15));
+      ++bases;
+    }
+    if (bases >= k) {
+      out.words.insert(out.words.end(), w.begin(), w.end());
+      out.hlen.push_back(hend - s);
+      out.heads.append(d + s, hend - s);
+    }
+    s = e;
+  }
+}
+
+}  // namespace
+
+extern "C" int r2m_fasta_reads(const char *data, size_t len, int k, int nthreads, r2m_reads **out) {
+  if (!out) return r2m::fail(R2M_EINVAL, "out is null");
+  *out = nullptr;
+  if (k < 1) return r2m::fail(R2M_EINVAL, "k must be >= 1");
+  if (!data && len) return r2m::fail(R2M_EINVAL, "data is null");
+  r2m_reads *r = new r2m_reads();
+  r->k = k;
+  r->W = (k + 15) / 16;
+  r->hoff.push_back(0);
+  if (len == 0) {
+    *out = r;
+    return R2M_OK;
+  }
+  if (nthreads < 1) nthreads = 1;
+  if (len < (size_t)(1 << 22)) nthreads = 1;
+  // split points at record starts
+  std::vector<size_t> cuts;
+  cuts.push_back(next_rec(data, 0, len));
+  for (int t = 1; t < nthreads; ++t) {
+    size_t guess = len * (size_t)t / (size_t)nthreads;
+    if (guess <= cuts.back()) continue;
+    size_t c = next_rec(data, guess, len);
+    if (c > cuts.back() && c < len) cuts.push_back(c);
+  }
+  cuts.push_back(len);
+  size_t np = cuts.size() - 1;
+  std::vector<Part> parts(np);
+  if (np == 1) {
+    parse_range(data, len, cuts[0], cuts[1], k, parts[0]);
+  } else {
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < np; ++i)
+      th.emplace_back(parse_range, data, len, cuts[i], cuts[i + 1], k, std::ref(parts[i]));
+    for (auto &t : th) t.join();
+  }
+  for (size_t i = 0; i < np; ++i) {
+    Part &p = parts[i];
+    r->words.insert(r->words.end(), p.words.begin(), p.words.end());
+    size_t off = 0;
+    for (size_t j = 0; j < p.hlen.size(); ++j) {
+      r->heads.append(p.heads, off, p.hlen[j]);
+      off += p.hlen[j];
+      r->hoff.push_back(r->heads.size());
+    }
+    if (p.stop) break;  // parse ends at an unterminated header line
+  }
+  *out = r;
+  return R2M_OK;
+}
+
+extern "C" int64_t r2m_reads_count(const r2m_reads *r) {
+  return r ? (int64_t)(r->hoff.size() - 1) : 0;
+}
+
+extern "C" const uint32_t *r2m_reads_words(const r2m_reads *r) {
+  return (r && !r->words.empty()) ? r->words.data() : nullptr;
+}
+
+extern "C" const char *r2m_reads_header(const r2m_reads *r, int64_t i, size_t *len) {
+  if (!r || i < 0 || i >= r2m_reads_count(r)) {
+    if (len) *len = 0;
+    return nullptr;
+  }
+  if (len) *len = r->hoff[i + 1] - r->hoff[i];
+  return r->heads.data() + r->hoff[i];
+}
+
+extern "C" void r2m_reads_free(r2m_reads *r) { delete r; }

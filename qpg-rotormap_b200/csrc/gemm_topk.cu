@@ -1,0 +1,687 @@
+// gemm_topk.cu -- the read x index similarity search: a persistent tcgen05
+// fp8 GEMM whose epilogue is a streaming per-row top-k, plus the merge of
+// the per-split partial lists and the engine object behind the C ABI.
+//
+// Replaces the reference's chunk loop batch_gemm_topk!
+// (RotorMap/search/engine_fp8.jl:399-437): cuBLASLt fp8 GEMM into an fp16 C
+// chunk in HBM (gemm/fp8_lt.jl:128-168) followed by seg_rowtopk_merge_kernel!
+// (gemm/topk_kernels.jl:213-329).  Here the score tile lives only in TMEM.
+//
+// Kernel structure (one CTA per SM, 192 threads):
+//   warp 0      TMA producer: A tile (128 reads x 128 B of K) and B tile
+//               (256 index columns x 128 B) per stage, 128-byte swizzle,
+//               4-stage mbarrier ring, no multicast.
+//   warp 1      TMEM owner + MMA issuer: tcgen05.mma kind::f8f6f4,
+//               M=128 N=256 K=32, fp32 accumulators double-buffered in TMEM
+//               (2 x 256 of the 512 columns).
+//   warps 2..5  epilogue: one thread per read row (TMEM lane); tcgen05.ld of
+//               32 columns at a time, score transform (fp16 rounding /
+//               column scale), chunk max vs the row's threshold, and
+//               insertion into a register reservoir of the top KT (score
+//               desc, column asc).
+// Work unit = (read tile of 128 rows, column split); each unit streams its
+// split's column tiles and leaves a sorted partial list per row; a second
+// kernel merges the splits.  Every mbarrier wait is bounded; a wait that
+// gives up raises a shared abort flag, records a code in the device error
+// word and the CTA drains its in-flight work before freeing TMEM.
+#include <float.h>
+#include <limits.h>
+
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace r2m {
+
+constexpr int BM = 128;           // read rows per tile (TMEM lanes)
+constexpr int BN = 256;           // index columns per tile (TMEM fp32 columns)
+constexpr int BK = 128;           // K bytes per stage (one 128-byte swizzle row)
+constexpr int STAGES = 4;
+constexpr int A_STAGE = BM * BK;  // 16 KiB
+constexpr int B_STAGE = BN * BK;  // 32 KiB
+constexpr int THREADS = 192;
+constexpr int TMEM_COLS = 512;
+constexpr long long WAIT_LIMIT = 4000000000LL;  // clock cycles (~2 s)
+constexpr int MAX_SPLITS = 128;
+
+struct GemmArgs {
+  int nb;
+  int num_m_tiles;
+  long long N;
+  int n_tiles;
+  int splits;
+  int num_kb;
+  int score_mode;
+  int mpad;  // num_m_tiles * BM (partial-list row stride)
+  const float *scaleB;
+  float *part_vals;
+  int *part_cols;
+  uint32_t *err;
+};
+
+__device__ __forceinline__ int split_lo(int s, int n_tiles, int splits) {
+  return (int)(((long long)s * n_tiles) / splits);
+}
+
+__device__ __forceinline__ float round_f16(float x) { return __half2float(__float2half_rn(x)); }
+
+// Reservoir of the best KT (value, column) pairs; order: larger value first,
+// equal values -> smaller column first.  `thr`/`mc` track the worst entry.
+template <int KT>
+struct Reservoir {
+  float v[KT];
+  int c[KT];
+  float thr;
+  int mc;
+  int minpos;
+
+  __device__ __forceinline__ void reset() {
+#pragma unroll
+    for (int i = 0; i < KT; ++i) {
+      v[i] = -INFINITY;
+      c[i] = INT_MAX;
+    }
+    thr = -INFINITY;
+    mc = INT_MAX;
+    minpos = 0;
+  }
+  // Called only with x > thr: columns arrive in increasing order, so a tie
+  // with the worst entry never displaces it.
+  __device__ __forceinline__ void insert(float x, int col) {
+#pragma unroll
+    for (int i = 0; i < KT; ++i)
+      if (i == minpos) {
+        v[i] = x;
+        c[i] = col;
+      }
+    float t = v[0];
+    int tc = c[0], tp = 0;
+#pragma unroll
+    for (int i = 1; i < KT; ++i) {
+      bool worse = (v[i] < t) || (v[i] == t && c[i] > tc);
+      t = worse ? v[i] : t;
+      tc = worse ? c[i] : tc;
+      tp = worse ? i : tp;
+    }
+    thr = t;
+    mc = tc;
+    minpos = tp;
+  }
+  __device__ __forceinline__ void sort_desc() {
+#pragma unroll
+    for (int i = 0; i < KT; ++i) {
+#pragma unroll
+      for (int j = KT - 1; j > i; --j) {
+        bool swap = (v[j] > v[j - 1]) || (v[j] == v[j - 1] && c[j] < c[j - 1]);
+        float tv = swap ? v[j] : v[j - 1];
+        int tcol = swap ? c[j] : c[j - 1];
+        v[j] = swap ? v[j - 1] : v[j];
+        c[j] = swap ? c[j - 1] : c[j];
+        v[j - 1] = tv;
+        c[j - 1] = tcol;
+      }
+    }
+  }
+};
+
+template <int KT>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_gemm_topk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem =
+      reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + STAGES * A_STAGE;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sB + STAGES * B_STAGE);
+  uint64_t *empty = full + STAGES;
+  uint64_t *acc_full = empty + STAGES;
+  uint64_t *acc_empty = acc_full + 2;
+  uint64_t *drain = acc_empty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // 128 x 33 floats
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 4);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int num_units = g.num_m_tiles * g.splits;
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      long long issued = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; ok && u < num_units; u += gridDim.x) {
+        const int mt = u % g.num_m_tiles, sp = u / g.num_m_tiles;
+        const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
+        for (int t = t0; ok && t < t1; ++t) {
+          for (int kb = 0; kb < g.num_kb; ++kb) {
+            if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, abort_flag, WAIT_LIMIT)) {
+              if (!*abort_flag) atomicExch(g.err, kErrTimeoutEmpty);
+              *abort_flag = 1;
+              ok = false;
+              break;
+            }
+            mbar_arrive_expect_tx(&full[stage], A_STAGE + B_STAGE);
+            tma_load_2d(sA + stage * A_STAGE, &tmA, &full[stage], kb * BK, mt * BM);
+            tma_load_2d(sB + stage * B_STAGE, &tmB, &full[stage], kb * BK, t * BN);
+            ++issued;
+            if (++stage == STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+        }
+      }
+      if (!ok) {
+        // let the copies already issued land before the CTA can exit
+        int nlast = issued < STAGES ? (int)issued : STAGES;
+        for (int j = 1; j <= nlast; ++j) {
+          int s = stage - j;
+          uint32_t ph = phase;
+          if (s < 0) {
+            s += STAGES;
+            ph ^= 1u;
+          }
+          long long t0 = clock64();
+          while (!mbar_try_wait(&full[s], ph) && clock64() - t0 < WAIT_LIMIT) {
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = idesc_e4m3_f32(BM, BN);
+      int stage = 0;
+      uint32_t phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; ok && u < num_units; u += gridDim.x) {
+        const int sp = u / g.num_m_tiles;
+        const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
+        for (int t = t0; ok && t < t1; ++t) {
+          if (!mbar_wait_bounded(&acc_empty[acc], acc_phase ^ 1u, abort_flag, WAIT_LIMIT)) {
+            if (!*abort_flag) atomicExch(g.err, kErrTimeoutAccEmpty);
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+          for (int kb = 0; kb < g.num_kb; ++kb) {
+            if (!mbar_wait_bounded(&full[stage], phase, abort_flag, WAIT_LIMIT)) {
+              if (!*abort_flag) atomicExch(g.err, kErrTimeoutFull);
+              *abort_flag = 1;
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA + stage * A_STAGE);
+            const uint32_t b0 = smem_u32(sB + stage * B_STAGE);
+#pragma unroll
+            for (int kk = 0; kk < BK / 32; ++kk) {
+              mma_f8(d_tmem, smem_desc_sw128(a0 + kk * 32), smem_desc_sw128(b0 + kk * 32), idesc,
+                     (kb | kk) != 0 ? 1u : 0u);
+            }
+            mma_commit(&empty[stage]);
+            if (++stage == STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+          if (!ok) break;
+          mma_commit(&acc_full[acc]);
+          acc ^= 1;
+          if (acc == 0) acc_phase ^= 1u;
+        }
+      }
+      // every MMA issued by this thread has completed once `drain` flips
+      mma_commit(drain);
+      long long t0 = clock64();
+      while (!mbar_try_wait(drain, 0) && clock64() - t0 < WAIT_LIMIT) {
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------ epilogue (top-k)
+    const int quarter = warp & 3;  // TMEM lanes [32*quarter, 32*quarter+32)
+    const int row_in_tile = quarter * 32 + lane;
+    float *scratch = scratch_all + (threadIdx.x - 64) * 33;
+    const bool f16 = g.score_mode == R2M_SCORE_F16;
+    const bool scaled = g.score_mode == R2M_SCORE_SCALED;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    Reservoir<KT> R;
+    for (int u = blockIdx.x; ok && u < num_units; u += gridDim.x) {
+      const int mt = u % g.num_m_tiles, sp = u / g.num_m_tiles;
+      const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
+      R.reset();
+      for (int t = t0; t < t1; ++t) {
+        bool w = mbar_wait_bounded(&acc_full[acc], acc_phase, abort_flag, WAIT_LIMIT);
+        if (__any_sync(FULL, !w)) {
+          if (lane == 0 && !*abort_flag) atomicExch(g.err, kErrTimeoutAccFull);
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
+        const long long colbase = (long long)t * BN;
+        const bool tail = colbase + BN > g.N;
+#pragma unroll 1
+        for (int ch = 0; ch < BN / 32; ++ch) {
+          float v[32];
+          __syncwarp();
+          tmem_ld32(taddr + ch * 32, v);
+          tmem_wait_ld();
+          const long long c0 = colbase + ch * 32;
+          if (scaled) {
+            if (!tail) {
+              const float4 *sb = reinterpret_cast<const float4 *>(g.scaleB + c0);
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                float4 s4 = __ldg(sb + q);
+                v[4 * q] *= s4.x;
+                v[4 * q + 1] *= s4.y;
+                v[4 * q + 2] *= s4.z;
+                v[4 * q + 3] *= s4.w;
+              }
+            } else {
+#pragma unroll
+              for (int j = 0; j < 32; ++j) v[j] = (c0 + j < g.N) ? v[j] * __ldg(g.scaleB + c0 + j) : v[j];
+            }
+          }
+          if (tail) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j >= g.N) v[j] = -INFINITY;
+          }
+          float mx = v[0];
+#pragma unroll
+          for (int j = 1; j < 32; ++j) mx = fmaxf(mx, v[j]);
+          if (f16) mx = round_f16(mx);
+          if (mx > R.thr) {
+            // rare path: stage the chunk and insert its survivors one by one
+#pragma unroll
+            for (int j = 0; j < 32; ++j) scratch[j] = v[j];
+#pragma unroll 1
+            for (int j = 0; j < 32; ++j) {
+              float x = scratch[j];
+              if (f16) x = round_f16(x);
+              if (x > R.thr) R.insert(x, (int)(c0 + j));
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[acc]);
+        acc ^= 1;
+        if (acc == 0) acc_phase ^= 1u;
+      }
+      if (!ok) break;
+      R.sort_desc();
+      const int row = mt * BM + row_in_tile;
+      if (row < g.nb) {
+        float *pv = g.part_vals + ((size_t)sp * g.mpad + row) * KT;
+        int *pc = g.part_cols + ((size_t)sp * g.mpad + row) * KT;
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          pv[j] = R.v[j];
+          pc[j] = R.c[j];
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, TMEM_COLS);
+  }
+}
+
+// Merge the per-split sorted lists of every row into its final top-k:
+// one warp per row, k rounds of a warp arg-max over the list heads.
+__global__ void k_merge_splits(const float *__restrict__ pv, const int *__restrict__ pc, int splits,
+                               int mpad, int KT, int nb, int k, int score_mode,
+                               const float *__restrict__ scaleA, float *out_v, int *out_l) {
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= nb) return;
+  const unsigned FULL = 0xFFFFFFFFu;
+  constexpr int PER = MAX_SPLITS / 32;
+  int head[PER];
+  float hv[PER];
+  int hc[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    int s = lane + 32 * q;
+    head[q] = 0;
+    if (s < splits) {
+      size_t b = ((size_t)s * mpad + row) * KT;
+      hv[q] = pv[b];
+      hc[q] = pc[b];
+    } else {
+      hv[q] = -INFINITY;
+      hc[q] = INT_MAX;
+    }
+  }
+  const float sa = (score_mode == R2M_SCORE_SCALED) ? scaleA[row] : 1.0f;
+  for (int r = 0; r < k; ++r) {
+    float bv = hv[0];
+    int bc = hc[0], bq = 0;
+#pragma unroll
+    for (int q = 1; q < PER; ++q) {
+      bool better = (hv[q] > bv) || (hv[q] == bv && hc[q] < bc);
+      bv = better ? hv[q] : bv;
+      bc = better ? hc[q] : bc;
+      bq = better ? q : bq;
+    }
+    float wv = bv;
+    int wc = bc, wl = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      float ov = __shfl_xor_sync(FULL, wv, o);
+      int oc = __shfl_xor_sync(FULL, wc, o);
+      int ol = __shfl_xor_sync(FULL, wl, o);
+      bool better = (ov > wv) || (ov == wv && oc < wc) || (ov == wv && oc == wc && ol < wl);
+      wv = better ? ov : wv;
+      wc = better ? oc : wc;
+      wl = better ? ol : wl;
+    }
+    if (lane == 0) {
+      bool empty = (wv == -INFINITY) || wc == INT_MAX;
+      out_v[(size_t)row * k + r] = empty ? -INFINITY : wv * sa;
+      out_l[(size_t)row * k + r] = empty ? 0 : wc + 1;
+    }
+    if (lane == wl) {
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        if (q == bq) {
+          int s = lane + 32 * q;
+          int h = ++head[q];
+          if (h < KT) {
+            size_t b = ((size_t)s * mpad + row) * KT + h;
+            hv[q] = pv[b];
+            hc[q] = pc[b];
+          } else {
+            hv[q] = -INFINITY;
+            hc[q] = INT_MAX;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------------ host
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int get_encode_fn(EncodeTiledFn *fn) {
+  static std::mutex mu;
+  static EncodeTiledFn cached = nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!cached) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+      return fail(R2M_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    cached = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  *fn = cached;
+  return R2M_OK;
+}
+
+// 2-D uint8 tensor of `rows` x `cols` bytes (row stride = cols), box
+// `box_rows` x 128 bytes, 128-byte swizzle, zero fill outside.
+static int make_map(CUtensorMap *map, const void *base, long long rows, int cols, int box_rows) {
+  EncodeTiledFn fn;
+  int rc = get_encode_fn(&fn);
+  if (rc) return rc;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box,
+                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(R2M_ECUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
+  return R2M_OK;
+}
+
+static int pick_kt(int k) {
+  if (k <= 8) return 8;
+  if (k <= 16) return 16;
+  if (k <= 20) return 20;
+  if (k <= 32) return 32;
+  return 64;
+}
+
+static size_t gemm_smem_bytes() {
+  return 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + (2 * STAGES + 5) * 8 + 16 +
+         (size_t)BM * 33 * sizeof(float);
+}
+
+// Column splits for a given number of read tiles: enough units to keep
+// every CTA busy, chosen to minimise the last-wave imbalance.
+static int choose_splits(int m_tiles, int n_tiles, int ctas, int forced) {
+  if (forced > 0) {
+    int s = forced;
+    if (s > n_tiles) s = n_tiles;
+    if (s > MAX_SPLITS) s = MAX_SPLITS;
+    return s < 1 ? 1 : s;
+  }
+  int smin = (4 * ctas + m_tiles - 1) / m_tiles;
+  if (smin < 1) smin = 1;
+  int cap = n_tiles < MAX_SPLITS ? n_tiles : MAX_SPLITS;
+  if (smin > cap) smin = cap;
+  int best = smin;
+  double best_eff = -1.0;
+  for (int s = smin; s <= cap && s <= 2 * smin; ++s) {
+    long long units = (long long)m_tiles * s;
+    long long waves = (units + ctas - 1) / ctas;
+    double eff = (double)units / (double)(waves * ctas);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = s;
+    }
+  }
+  return best;
+}
+
+template <int KT>
+static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmArgs &g, int ctas,
+                       cudaStream_t st) {
+  size_t smem = gemm_smem_bytes();
+  static bool attr_set[8] = {false};
+  int slot = KT == 8 ? 0 : KT == 16 ? 1 : KT == 20 ? 2 : KT == 32 ? 3 : 4;
+  if (!attr_set[slot]) {
+    R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[slot] = true;
+  }
+  k_gemm_topk<KT><<<ctas, THREADS, smem, st>>>(mA, mB, g);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
+
+}  // namespace r2m
+
+using namespace r2m;
+
+struct r2m_engine {
+  const uint8_t *B;
+  const float *scaleB;
+  int rdim;
+  long long N;
+  int k, KT;
+  int rows_cap;
+  int score_mode;
+  int ctas;
+  int forced_splits;
+  int n_tiles;
+  CUtensorMap mapB;
+  float *part_vals;
+  int *part_cols;
+  size_t part_lists;  // capacity in lists (rows x splits)
+  uint32_t *err;
+};
+
+extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int rdim, int64_t N, int k,
+                                 int rows_cap, int score_mode, const r2m_tuning *tune,
+                                 r2m_engine **out) {
+  R2M_REQUIRE(out != nullptr, "out is null");
+  *out = nullptr;
+  R2M_REQUIRE(d_B != nullptr, "B is null");
+  R2M_REQUIRE(rdim >= 16 && rdim % 16 == 0, "rdim must be a positive multiple of 16");
+  R2M_REQUIRE(N >= 1 && N <= (1LL << 31) - 1 - BN, "N out of range");
+  R2M_REQUIRE(k >= 1 && k <= 64 && k <= N, "need 1 <= k <= min(N, 64)");
+  R2M_REQUIRE(rows_cap >= 1, "rows_cap must be >= 1");
+  R2M_REQUIRE(score_mode >= R2M_SCORE_F16 && score_mode <= R2M_SCORE_SCALED, "bad score_mode");
+  R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || d_scaleB, "scaled scores need scaleB");
+  R2M_REQUIRE((reinterpret_cast<uintptr_t>(d_B) & 15) == 0, "B must be 16-byte aligned");
+  R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || (reinterpret_cast<uintptr_t>(d_scaleB) & 15) == 0,
+              "scaleB must be 16-byte aligned");
+  int rc = r2m_device_check();
+  if (rc) return rc;
+  r2m_engine *e = new r2m_engine();
+  e->B = d_B;
+  e->scaleB = d_scaleB;
+  e->rdim = rdim;
+  e->N = N;
+  e->k = k;
+  e->KT = pick_kt(k);
+  e->rows_cap = rows_cap;
+  e->score_mode = score_mode;
+  e->ctas = (tune && tune->ctas > 0) ? tune->ctas : sm_count();
+  e->forced_splits = (tune && tune->splits > 0) ? tune->splits : 0;
+  e->n_tiles = (int)((N + BN - 1) / BN);
+  rc = make_map(&e->mapB, d_B, N, rdim, BN);
+  if (rc) {
+    delete e;
+    return rc;
+  }
+  // workspace: the largest (read tiles x splits) any batch height can ask for
+  int mt_cap = (rows_cap + BM - 1) / BM;
+  size_t lists = 0;
+  for (int mt = 1; mt <= mt_cap; ++mt) {
+    int s = choose_splits(mt, e->n_tiles, e->ctas, e->forced_splits);
+    size_t l = (size_t)s * mt * BM;
+    if (l > lists) lists = l;
+  }
+  e->part_lists = lists;
+  cudaError_t ce = cudaMalloc(&e->part_vals, lists * e->KT * sizeof(float));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->part_cols, lists * e->KT * sizeof(int));
+  if (ce != cudaSuccess) {
+    cudaFree(e->part_vals);
+    delete e;
+    return fail(R2M_ENOMEM, "engine workspace allocation failed");
+  }
+  rc = device_error_word(&e->err);
+  if (rc) {
+    cudaFree(e->part_vals);
+    cudaFree(e->part_cols);
+    delete e;
+    return rc;
+  }
+  *out = e;
+  return R2M_OK;
+}
+
+extern "C" int r2m_engine_destroy(r2m_engine *eng) {
+  if (!eng) return R2M_OK;
+  cudaFree(eng->part_vals);
+  cudaFree(eng->part_cols);
+  delete eng;
+  return R2M_OK;
+}
+
+extern "C" int64_t r2m_engine_workspace_bytes(const r2m_engine *eng) {
+  if (!eng) return 0;
+  return (int64_t)(eng->part_lists * eng->KT * (sizeof(float) + sizeof(int)));
+}
+
+extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const float *d_scaleA, int nb,
+                                   float *d_vals, int32_t *d_locs, r2m_stream_t stream) {
+  R2M_REQUIRE(eng != nullptr, "engine is null");
+  R2M_REQUIRE(nb >= 0 && nb <= eng->rows_cap, "nb must be in 0..rows_cap");
+  if (nb == 0) return R2M_OK;
+  R2M_REQUIRE(d_A && d_vals && d_locs, "null pointer");
+  R2M_REQUIRE((reinterpret_cast<uintptr_t>(d_A) & 15) == 0, "A must be 16-byte aligned");
+  R2M_REQUIRE(eng->score_mode != R2M_SCORE_SCALED || d_scaleA, "scaled scores need scaleA");
+  cudaStream_t st = as_stream(stream);
+  CUtensorMap mapA;
+  int rc = make_map(&mapA, d_A, nb, eng->rdim, BM);
+  if (rc) return rc;
+  GemmArgs g;
+  g.nb = nb;
+  g.num_m_tiles = (nb + BM - 1) / BM;
+  g.N = eng->N;
+  g.n_tiles = eng->n_tiles;
+  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, eng->ctas, eng->forced_splits);
+  g.num_kb = (eng->rdim + BK - 1) / BK;
+  g.score_mode = eng->score_mode;
+  g.mpad = g.num_m_tiles * BM;
+  g.scaleB = eng->scaleB;
+  g.part_vals = eng->part_vals;
+  g.part_cols = eng->part_cols;
+  g.err = eng->err;
+  if ((size_t)g.splits * g.mpad > eng->part_lists) return fail(R2M_ESTATE, "engine workspace too small");
+  long long units = (long long)g.num_m_tiles * g.splits;
+  int ctas = (int)(units < eng->ctas ? units : eng->ctas);
+  switch (eng->KT) {
+    case 8: rc = launch_gemm<8>(mapA, eng->mapB, g, ctas, st); break;
+    case 16: rc = launch_gemm<16>(mapA, eng->mapB, g, ctas, st); break;
+    case 20: rc = launch_gemm<20>(mapA, eng->mapB, g, ctas, st); break;
+    case 32: rc = launch_gemm<32>(mapA, eng->mapB, g, ctas, st); break;
+    default: rc = launch_gemm<64>(mapA, eng->mapB, g, ctas, st); break;
+  }
+  if (rc) return rc;
+  const int warps = 8;
+  k_merge_splits<<<(nb + warps - 1) / warps, 32 * warps, 0, st>>>(
+      eng->part_vals, eng->part_cols, g.splits, g.mpad, eng->KT, nb, eng->k, eng->score_mode, d_scaleA,
+      d_vals, d_locs);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}

@@ -1,0 +1,110 @@
+"""ctypes binding of librotormap_b200.so (the C ABI declared in include/r2m.h).
+
+The library is built in-tree (qpg-rotormap_b200/build.py).  There is no
+fallback: if the shared object is missing or no sm_100 device is present,
+every entry point raises R2MError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(os.environ.get(
+    "R2M_LIB", Path(__file__).resolve().parent.parent / "lib" / "librotormap_b200.so"))
+
+R2M_OK, R2M_EINVAL, R2M_ECUDA, R2M_ENOMEM, R2M_ETIMEOUT, R2M_ESTATE, R2M_EIO = 0, -1, -2, -3, -4, -5, -6
+OUT_F32, OUT_F16, OUT_E4M3, OUT_E4M3_SCALED = 0, 1, 2, 3
+SCORE_F16, SCORE_F32, SCORE_SCALED = 0, 1, 2
+
+_CODES = {R2M_EINVAL: "EINVAL", R2M_ECUDA: "ECUDA", R2M_ENOMEM: "ENOMEM", R2M_ETIMEOUT: "ETIMEOUT",
+          R2M_ESTATE: "ESTATE", R2M_EIO: "EIO"}
+
+
+class R2MError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"r2m error {_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("splits", ctypes.c_int), ("ctas", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
+# (name, restype, argtypes) of every symbol in include/r2m.h
+P = ctypes.c_void_p
+I = ctypes.c_int
+I64 = ctypes.c_int64
+SZ = ctypes.c_size_t
+SIGNATURES = [
+    ("r2m_last_error", ctypes.c_char_p, []),
+    ("r2m_version", I, []),
+    ("r2m_device_check", I, []),
+    ("r2m_check_device_error", I, [P]),
+    ("r2m_encode_frag_real_batch", I, [P, I, P, P, P, I64, I, I, I, I, I, P]),
+    ("r2m_revcomp_frag_words", I, [P, P, I, I64, P]),
+    ("r2m_encode_ref_windows", I, [P, I, P, P, P, P, I64, I64, I, I, I, I, I, P]),
+    ("r2m_f32_to_e4m3", I, [P, P, I64, P]),
+    ("r2m_f16_to_e4m3", I, [P, P, I64, P]),
+    ("r2m_engine_create", I, [P, P, I, I64, I, I, I, ctypes.POINTER(Tuning), ctypes.POINTER(P)]),
+    ("r2m_engine_destroy", I, [P]),
+    ("r2m_engine_workspace_bytes", I64, [P]),
+    ("r2m_batch_gemm_topk", I, [P, P, P, I, P, P, P]),
+    ("r2m_fasta_reads", I, [ctypes.c_char_p, SZ, I, I, ctypes.POINTER(P)]),
+    ("r2m_reads_count", I64, [P]),
+    ("r2m_reads_words", P, [P]),
+    ("r2m_reads_header", P, [P, I64, ctypes.POINTER(SZ)]),
+    ("r2m_reads_free", None, [P]),
+]
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib() -> ctypes.CDLL:
+    """Load the library once; raises R2MError when it has not been built."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not LIB_PATH.exists():
+                    raise R2MError(R2M_ESTATE, f"{LIB_PATH} not found: build it with "
+                                               "`python qpg-rotormap_b200/build.py`")
+                L = ctypes.CDLL(str(LIB_PATH))
+                for name, res, args in SIGNATURES:
+                    fn = getattr(L, name)
+                    fn.restype = res
+                    fn.argtypes = args
+                _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != R2M_OK:
+        msg = lib().r2m_last_error()
+        raise R2MError(rc, msg.decode() if msg else "")
+
+
+def ptr(t) -> int | None:
+    """Device/host address of a torch tensor or numpy array (None -> NULL)."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+def stream_handle(stream=None) -> int | None:
+    """cudaStream_t of a torch stream (default: torch's current stream)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def require_device() -> None:
+    """Fail loudly unless an sm_100 GPU is current (no CPU fallback exists)."""
+    import torch
+    if not torch.cuda.is_available():
+        raise R2MError(R2M_ESTATE, "no CUDA device: librotormap_b200 runs on B200 (sm_100a) only")
+    check(lib().r2m_device_check())

@@ -1,0 +1,220 @@
+"""fp8 search engine (mirror of RotorMap/search/engine_fp8.jl and engine_compact.jl).
+
+TopKEngine wraps the library's fused tcgen05 GEMM + top-k engine
+(r2m_engine_*).  The reference's chunk width `w`, top-k segments `segs` and
+double-buffered C chunks have no counterpart: scores never leave TMEM.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import Tuning, check, lib, ptr, stream_handle
+from .encoder import RopeEncoder, encode_frag_real_batch, f16_to_f8
+from .fasta import FastaFragments, fasta_reads
+
+_MODES = {"f16": _lib.SCORE_F16, "f32": _lib.SCORE_F32, "scaled": _lib.SCORE_SCALED}
+
+
+@dataclass
+class TopKBatch:
+    """One batch of results (engine_fp8.jl:265-271): vals (nb, k) float32
+    descending, locs (nb, k) int32 1-based global column ids, norms (nb, m),
+    heads, first (1-based global index of the batch's first read)."""
+    vals: np.ndarray
+    locs: np.ndarray
+    norms: np.ndarray
+    heads: list
+    first: int
+
+
+def padmul() -> int:
+    """Batch-height multiple of the engine (padmul, engine_fp8.jl:275): the
+    fused kernel takes any height, so 1."""
+    return 1
+
+
+class TopKEngine:
+    """TopKEngine(B; k, rows_cap, ...) (engine_fp8.jl:290-337).
+
+    B: (N, rdim) uint8 e4m3 CUDA tensor (the reference's (rdim, N)
+    column-major embeds8).  score: "f16" (reference cout = :f16, default),
+    "f32" (cout = :f32) or "scaled" (per-row / per-column fp32 scales; needs
+    scaleB).  The engine owns an e4m3 staging buffer `a8` (rows_cap, rdim) and
+    its split workspace; B and the outputs belong to the caller.
+    """
+
+    def __init__(self, B: torch.Tensor, k: int = 20, w: int | None = None, rows_cap: int = 8192,
+                 segs: int | None = None, score: str = "f16", scaleB: torch.Tensor | None = None,
+                 splits: int = 0, ctas: int = 0):
+        _lib.require_device()
+        if B.dtype != torch.uint8 or B.dim() != 2 or not B.is_cuda or not B.is_contiguous():
+            raise ValueError("B must be a contiguous (N, rdim) uint8 CUDA tensor")
+        N, rdim = B.shape
+        if not (1 <= k <= N):
+            raise ValueError(f"need 1 <= k <= N (got k = {k}, N = {N})")
+        if score not in _MODES:
+            raise ValueError("score must be 'f16', 'f32' or 'scaled'")
+        if rdim % 16:
+            raise ValueError(f"rdim must be a multiple of 16 (got {rdim})")
+        self.B, self.k, self.rows_cap, self.score = B, k, rows_cap, score
+        self.scaleB = scaleB
+        self.N, self.rdim = N, rdim
+        self.a8 = torch.zeros((rows_cap, rdim), dtype=torch.uint8, device=B.device)
+        self.scaleA = torch.ones((rows_cap,), dtype=torch.float32, device=B.device)
+        tune = Tuning(splits, ctas)
+        h = ctypes.c_void_p()
+        check(lib().r2m_engine_create(ptr(B), ptr(scaleB), rdim, N, k, rows_cap, _MODES[score],
+                                      ctypes.byref(tune), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(lib().r2m_engine_workspace_bytes(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().r2m_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, A8: torch.Tensor, nb: int | None = None, scaleA: torch.Tensor | None = None,
+               D_val: torch.Tensor | None = None, D_loc: torch.Tensor | None = None, stream=None):
+        """Top-k of rows 0..nb-1 of A8 against B -> (D_val (nb, k), D_loc (nb, k))."""
+        nb = A8.shape[0] if nb is None else nb
+        if nb > self.rows_cap:
+            raise ValueError(f"batch height {nb} > engine rows_cap {self.rows_cap}")
+        if A8.dtype != torch.uint8 or A8.shape[1] != self.rdim or not A8.is_contiguous():
+            raise ValueError("A8 must be a contiguous (nb, rdim) uint8 tensor")
+        if self.score == "scaled" and scaleA is None:
+            raise ValueError("scaled scores need scaleA")
+        dev = self.B.device
+        if D_val is None:
+            D_val = torch.empty((nb, self.k), dtype=torch.float32, device=dev)
+        if D_loc is None:
+            D_loc = torch.empty((nb, self.k), dtype=torch.int32, device=dev)
+        check(lib().r2m_batch_gemm_topk(self._h, ptr(A8), ptr(scaleA), nb, ptr(D_val), ptr(D_loc),
+                                        stream_handle(stream)))
+        return D_val, D_loc
+
+
+def upload_fp16_as_f8(eng: TopKEngine, embeds, stream=None) -> torch.Tensor:
+    """upload_fp16_as_f8! (engine_fp8.jl:355-371): H2D an fp16 (nb, rdim) batch
+    and quantise it into the engine staging `a8` rows 0..nb-1."""
+    e = torch.as_tensor(embeds)
+    if e.dtype != torch.float16:
+        raise TypeError("embeds must be float16")
+    nb, rdim = e.shape
+    if rdim != eng.rdim or nb > eng.rows_cap:
+        raise ValueError("batch shape does not fit the engine staging")
+    d = e.to(eng.B.device, non_blocking=True).contiguous()
+    f16_to_f8(eng.a8[:nb], d, stream)
+    return eng.a8
+
+
+def batch_gemm_topk(D_val: torch.Tensor, D_loc: torch.Tensor, eng: TopKEngine, nb: int | None = None,
+                    A8: torch.Tensor | None = None, scaleA: torch.Tensor | None = None, stream=None):
+    """batch_gemm_topk! (engine_fp8.jl:399-437): top-k of the staged batch
+    (eng.a8 unless A8 is given) into D_val / D_loc (at least nb rows)."""
+    A = eng.a8 if A8 is None else A8
+    nb = A.shape[0] if nb is None else nb
+    sa = scaleA if scaleA is not None else (eng.scaleA if eng.score == "scaled" else None)
+    eng.search(A, nb, sa, D_val, D_loc, stream)
+    return D_val, D_loc
+
+
+# ------------------------------------------------------------------ flows
+
+
+def _batches(frags: FastaFragments, batch_size: int):
+    for b0 in range(0, len(frags), batch_size):
+        yield b0, frags.words[b0:b0 + batch_size], frags.heads[b0:b0 + batch_size]
+
+
+def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stream=None):
+    """topk_flow (engine_fp8.jl:498-547) over an iterable of
+    (first0, words (nb, W) uint32, heads) batches: encode on the GPU straight
+    to e4m3 (fp16-rounded, or per-row scaled for score = "scaled"), search,
+    and yield TopKBatch with host arrays."""
+    dev = eng.B.device
+    st = stream if stream is not None else torch.cuda.current_stream(dev)
+    scaled = eng.score == "scaled"
+    for first0, words, heads in source:
+        nb = words.shape[0]
+        if nb == 0:
+            continue
+        if nb > eng.rows_cap:
+            raise ValueError(f"batch height {nb} > engine rows_cap {eng.rows_cap}")
+        hw = torch.from_numpy(np.ascontiguousarray(words, dtype=np.uint32)).pin_memory()
+        with torch.cuda.stream(st):
+            dw = hw.to(dev, non_blocking=True).view(torch.int32)
+            norms = torch.empty((nb, re.m), dtype=torch.float32, device=dev)
+            a8 = eng.a8[:nb]
+            sa = eng.scaleA[:nb] if scaled else None
+            encode_frag_real_batch(a8, norms, re, dw, normalize, sa, st)
+            D_val, D_loc = eng.search(a8, nb, sa, stream=st)
+            vals = D_val.to("cpu", non_blocking=True)
+            locs = D_loc.to("cpu", non_blocking=True)
+            nrm = norms.to("cpu", non_blocking=True)
+        st.synchronize()
+        yield TopKBatch(vals.numpy(), locs.numpy(), nrm.numpy(), list(heads), first0 + 1)
+
+
+def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int | None = None,
+                     batch_size: int = 8192, rows_cap: int | None = None, normalize: int = 0,
+                     score: str = "f16", scaleB: torch.Tensor | None = None, parts: int | None = None,
+                     segs: int | None = None, engine: TopKEngine | None = None, stream=None):
+    """rope_topk_stream (engine_fp8.jl:576-594): FASTA -> encode -> fp8 GEMM +
+    top-k against the resident B -> TopKBatch per batch (file order)."""
+    if B.shape[1] != re.rdim:
+        raise ValueError(f"B is {tuple(B.shape)}; the encoder's real embedding dim is {re.rdim}")
+    frags = fasta_reads(file, k=re.k, parts=parts)
+    eng = engine or TopKEngine(B, k=k, rows_cap=rows_cap or batch_size, score=score, scaleB=scaleB)
+    yield from topk_flow(_batches(frags, batch_size), eng, re, normalize, stream)
+
+
+def resident_need(host_bytes: int, rows_cap: int, rdim: int, k: int = 20) -> int:
+    """_resident_need (engine_compact.jl:195-205) for this engine: B + the e4m3
+    staging + per-batch temps + the split workspace bound + slack."""
+    return int(host_bytes + rows_cap * rdim * 2 + rows_cap * 64 * k * 8 * 2 + 96 * 2 ** 20)
+
+
+def resident_fits(host_bytes: int, rows_cap: int, rdim: int, k: int = 20, device=None) -> bool:
+    """resident_fits (engine_compact.jl:238-242): the index plus the engine's
+    working set fits the device memory free right now."""
+    free, _ = torch.cuda.mem_get_info(device)
+    return resident_need(host_bytes, rows_cap, rdim, k) <= free
+
+
+def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size: int = 8192,
+                             rows_cap: int | None = None, normalize: int = 0, score: str = "f16",
+                             scaleB=None, resident: bool | None = None, **kw):
+    """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index.
+
+    A B200's 180 GB hold every index this path targets, so the auto policy
+    uploads B once (resident); an index that does not fit raises instead of
+    streaming it through a host ring."""
+    Bh = np.asarray(Bh) if not isinstance(Bh, torch.Tensor) else Bh
+    nbytes = Bh.nbytes if isinstance(Bh, np.ndarray) else Bh.numel()
+    cap = rows_cap or batch_size
+    if resident is None:
+        resident = resident_fits(nbytes, cap, re.rdim, k)
+    if not resident:
+        raise MemoryError("index + engine working set exceed free device memory "
+                          "(host-ring streaming is not part of this build)")
+    B = Bh if isinstance(Bh, torch.Tensor) and Bh.is_cuda else torch.from_numpy(np.ascontiguousarray(Bh)).cuda()
+    sb = None
+    if scaleB is not None:
+        sb = scaleB if isinstance(scaleB, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(scaleB))
+        sb = sb.cuda()
+    yield from rope_topk_stream(re, file, B, k=k, batch_size=batch_size, rows_cap=cap,
+                                normalize=normalize, score=score, scaleB=sb, **kw)

@@ -1,0 +1,338 @@
+"""Index build / save / load (mirror of RotorMap/index/build.jl and load.jl).
+
+The reference index is a Julia-serialized NamedTuple (format
+"indexreal.fp8.v1": embeds8 (rdim, 2*n_frag) e4m3 columns, norms (m, 2*n_frag),
+heads, starts (1-based), strand (0 fwd / 1 rc), k, kstep, s, m, c,
+normalize).  This module keeps those fields and that column layout; on disk it
+uses a flat container (magic "R2MIDX01", a JSON header, 64-byte aligned raw
+arrays) that numpy can memory-map, because Julia's Serialization format is
+not available to a C/Python host.
+
+Build: the host packs every record once into 2-bit words (each record starts
+on a word boundary and is followed by a zero guard word), lists the window
+starts (offsets 0, kstep, ... with the window fully inside the record,
+build.jl:291-324) and the GPU encodes the forward and reverse-complement
+window of every start straight into e4m3 index columns
+(r2m_encode_ref_windows), in the reference's per-batch [fwd | rc] column
+order (build.jl:640-660).
+"""
+from __future__ import annotations
+
+import json
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_handle
+from .encoder import RopeEncoder
+
+FP8_FORMAT = "indexreal.fp8.v1"          # load.jl:31
+SCALED_FORMAT = "indexreal.fp8scaled.v1"  # per-column scaled e4m3 (precision form)
+_MAGIC = b"R2MIDX01"
+
+_LUT = np.full(256, 2, dtype=np.uint8)  # reader.jl:21-28: junk / IUPAC -> G
+for _ch, _code in (("A", 0), ("C", 1), ("G", 2), ("T", 3), ("a", 0), ("c", 1), ("g", 2), ("t", 3)):
+    _LUT[ord(_ch)] = _code
+
+
+@dataclass
+class RefPack:
+    """Packed reference: verbatim headers, per-record word offset / base count."""
+    heads: list
+    word_off: np.ndarray   # int64, first word of each record in `words`
+    nbases: np.ndarray     # int64
+    words: np.ndarray      # uint32, all records + guard words
+
+
+def _pack_codes(codes: np.ndarray) -> np.ndarray:
+    n = codes.size
+    nw = (n + 15) // 16
+    pad = np.zeros(nw * 16, np.uint32)
+    pad[:n] = codes
+    sh = (2 * np.arange(16, dtype=np.uint32))[None, :]
+    return np.bitwise_or.reduce(pad.reshape(nw, 16) << sh, axis=1).astype(np.uint32)
+
+
+def pack_records(heads, codes_list) -> RefPack:
+    """Pack records given as 2-bit code arrays (one per record)."""
+    offs, nb, chunks = [], [], []
+    cur = 0
+    for codes in codes_list:
+        codes = np.asarray(codes, dtype=np.uint8)
+        w = _pack_codes(codes)
+        offs.append(cur)
+        nb.append(codes.size)
+        chunks.append(w)
+        chunks.append(np.zeros(1, np.uint32))  # guard word
+        cur += w.size + 1
+    words = np.concatenate(chunks) if chunks else np.zeros(1, np.uint32)
+    return RefPack(list(heads), np.array(offs, np.int64), np.array(nb, np.int64), words)
+
+
+def _record_spans(raw: bytes):
+    """(start, header_end, seq_lo, seq_hi) per record (build.jl:291-324 walk)."""
+    arr = np.frombuffer(raw, np.uint8)
+    n = arr.size
+    gt = np.flatnonzero(arr == 0x3E)
+    if gt.size:
+        prev = np.where(gt > 0, arr[np.maximum(gt - 1, 0)], 0x0A)
+        gt = gt[(gt == 0) | (prev == 0x0A) | (prev == 0x0D)]
+    nls = np.flatnonzero(arr == 0x0A)
+    spans = []
+    for i, s in enumerate(gt):
+        e = gt[i + 1] if i + 1 < gt.size else n
+        j = np.searchsorted(nls, s)
+        h = nls[j] if j < nls.size else n  # header line ends at the first '\n' (any later)
+        hend = h
+        if hend > s and arr[hend - 1] == 0x0D:
+            hend -= 1
+        spans.append((int(s), int(hend), int(h) + 1, int(e)))
+    return arr, spans
+
+
+def pack_reference(raw: bytes) -> RefPack:
+    """Parse a reference FASTA (bytes) and pack every record."""
+    arr, spans = _record_spans(raw)
+    heads, codes_list = [], []
+    for s, hend, lo, hi in spans:
+        heads.append(bytes(arr[s:hend]).decode("latin-1"))
+        body = arr[lo:hi] if lo < hi else arr[0:0]
+        body = body[(body != 0x0A) & (body != 0x0D)]
+        codes_list.append(_LUT[body])
+    return pack_records(heads, codes_list)
+
+
+def window_positions(pack: RefPack, k: int, kstep: int):
+    """Window starts fully inside each record: (pos, rec, start_1based)."""
+    pos, rec, st = [], [], []
+    for r, (wo, nbases) in enumerate(zip(pack.word_off, pack.nbases)):
+        if nbases < k:
+            continue
+        offs = np.arange(0, nbases - k + 1, kstep, dtype=np.int64)
+        pos.append(16 * wo + offs)
+        rec.append(np.full(offs.size, r, np.int32))
+        st.append(offs + 1)
+    if not pos:
+        return np.zeros(0, np.int64), np.zeros(0, np.int32), np.zeros(0, np.int64)
+    return np.concatenate(pos), np.concatenate(rec), np.concatenate(st)
+
+
+def batch_column_order(nwin: int, batch: int):
+    """Column -> (window, strand) under the per-batch [fwd block | rc block] layout."""
+    col_win = np.empty(2 * nwin, np.int64)
+    strand = np.empty(2 * nwin, np.uint8)
+    for b0 in range(0, nwin, batch):
+        nb = min(batch, nwin - b0)
+        c0 = 2 * b0
+        w = np.arange(b0, b0 + nb, dtype=np.int64)
+        col_win[c0:c0 + nb] = w
+        col_win[c0 + nb:c0 + 2 * nb] = w
+        strand[c0:c0 + nb] = 0
+        strand[c0 + nb:c0 + 2 * nb] = 1
+    return col_win, strand
+
+
+@dataclass
+class Index:
+    """The loaded/built index: reference NamedTuple fields + packed genome."""
+    format: str
+    source: str
+    k: int
+    kstep: int
+    s: int
+    m: int
+    c: int
+    normalize: int
+    n_frag: int
+    embeds8: object            # (N, rdim) uint8: torch CUDA tensor or numpy (host)
+    norms: np.ndarray          # (N, m) float32
+    rec_heads: list            # unique record headers (verbatim, with '>')
+    col_rec: np.ndarray        # (N,) int32 record of each column
+    starts: np.ndarray         # (N,) int64 1-based window start
+    strand: np.ndarray         # (N,) uint8
+    col_pos: np.ndarray        # (N,) int64 absolute base position in `genome`
+    genome: np.ndarray         # packed words of all records
+    rec_word_off: np.ndarray
+    rec_nbases: np.ndarray
+    batch_size: int = 8192
+    scales: object = None      # (N,) float32 column scales (scaled form only)
+    _heads: list = field(default=None, repr=False)
+
+    @property
+    def N(self) -> int:
+        return int(self.col_rec.size)
+
+    @property
+    def rdim(self) -> int:
+        return 2 * self.m * 4 ** self.c
+
+    @property
+    def encoder(self) -> RopeEncoder:
+        return RopeEncoder(k=self.k, s=self.s, m=self.m, c=self.c)
+
+    @property
+    def heads(self) -> list:
+        """Per-column verbatim record header (the reference's `heads` field)."""
+        if self._heads is None:
+            self._heads = [self.rec_heads[i] for i in self.col_rec]
+        return self._heads
+
+    @property
+    def scaled(self) -> bool:
+        return self.format == SCALED_FORMAT
+
+    def save(self, path) -> None:
+        save_index(self, path)
+
+
+def build_index(re: RopeEncoder, source, kstep: int | None = None, batch_size: int = 8192,
+                normalize: int = 0, scaled: bool = False, device=None, stream=None,
+                pack: RefPack | None = None) -> Index:
+    """build_index_matrix + _index_data_nt (build.jl:694-768), on the GPU.
+
+    source: a FASTA path or bytes (ignored when `pack` is given).  The
+    e4m3 columns stay on `device` (the resident database B).
+    """
+    if kstep is None:
+        kstep = max(re.k // 10, 1)
+    if kstep < 1 or batch_size < 1:
+        raise ValueError("kstep and batch_size must be >= 1")
+    _lib.require_device()
+    if pack is None:
+        raw = source if isinstance(source, (bytes, bytearray)) else open(source, "rb").read()
+        pack = pack_reference(bytes(raw))
+        src_name = "<bytes>" if isinstance(source, (bytes, bytearray)) else os.path.abspath(source)
+    else:
+        src_name = str(source)
+    pos, rec, st = window_positions(pack, re.k, kstep)
+    nwin = pos.size
+    col_win, strand = batch_column_order(nwin, batch_size)
+    N = 2 * nwin
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    B = torch.empty((N, re.rdim), dtype=torch.uint8, device=dev)
+    norms = torch.empty((N, re.m), dtype=torch.float32, device=dev)
+    scales = torch.empty((N,), dtype=torch.float32, device=dev) if scaled else None
+    if nwin:
+        g = torch.from_numpy(pack.words).to(dev)
+        p = torch.from_numpy(pos).to(dev)
+        kind = _lib.OUT_E4M3_SCALED if scaled else _lib.OUT_E4M3
+        check(lib().r2m_encode_ref_windows(ptr(B), kind, ptr(norms), ptr(scales), ptr(g), ptr(p), nwin,
+                                           batch_size, re.k, re.s, re.m, re.c, normalize,
+                                           stream_handle(stream)))
+        torch.cuda.current_stream(dev).synchronize() if stream is None else stream.synchronize()
+        del g, p
+    return Index(format=SCALED_FORMAT if scaled else FP8_FORMAT, source=src_name, k=re.k, kstep=kstep,
+                 s=re.s, m=re.m, c=re.c, normalize=normalize, n_frag=nwin, embeds8=B,
+                 norms=norms.cpu().numpy(), rec_heads=list(pack.heads),
+                 col_rec=rec[col_win] if nwin else np.zeros(0, np.int32),
+                 starts=st[col_win] if nwin else np.zeros(0, np.int64), strand=strand,
+                 col_pos=pos[col_win] if nwin else np.zeros(0, np.int64), genome=pack.words,
+                 rec_word_off=pack.word_off, rec_nbases=pack.nbases, batch_size=batch_size,
+                 scales=scales)
+
+
+# ------------------------------------------------------------------ file I/O
+
+_ARRAYS = ("embeds8", "norms", "col_rec", "starts", "strand", "col_pos", "genome", "rec_word_off",
+           "rec_nbases", "scales")
+
+
+def _host(a):
+    if a is None:
+        return None
+    if isinstance(a, torch.Tensor):
+        return a.detach().cpu().numpy()
+    return np.asarray(a)
+
+
+def save_index(idx: Index, path) -> None:
+    """run_save (build.jl:781-795) into the flat container (see module doc)."""
+    meta = dict(format=idx.format, source=idx.source, k=idx.k, kstep=idx.kstep, s=idx.s, m=idx.m,
+                c=idx.c, normalize=idx.normalize, fp8=True, n_frag=idx.n_frag,
+                batch_size=idx.batch_size, rec_heads=idx.rec_heads, arrays={})
+    arrays = {}
+    for name in _ARRAYS:
+        a = _host(getattr(idx, name))
+        if a is not None:
+            arrays[name] = np.ascontiguousarray(a)
+    off = 0
+    for name, a in arrays.items():
+        meta["arrays"][name] = dict(dtype=a.dtype.str, shape=list(a.shape), offset=off)
+        off += (a.nbytes + 63) // 64 * 64
+    hdr = json.dumps(meta).encode()
+    base = (len(_MAGIC) + 8 + len(hdr) + 63) // 64 * 64
+    with open(path, "wb") as f:
+        f.write(_MAGIC)
+        f.write(np.uint64(len(hdr)).tobytes())
+        f.write(hdr)
+        f.write(b"\0" * (base - len(_MAGIC) - 8 - len(hdr)))
+        pos = 0
+        for name, a in arrays.items():
+            o = meta["arrays"][name]["offset"]
+            if o > pos:
+                f.write(b"\0" * (o - pos))
+                pos = o
+            f.write(a.tobytes())
+            pos += a.nbytes
+
+
+def load_index(path, device=None, mmap: bool = True) -> Index:
+    """load_index (load.jl:49-73): structural checks, normalize == 0 required.
+
+    embeds8 stays on the host (memory-mapped) unless `device` is given, in
+    which case it is uploaded once (index_database, load.jl:156-161).
+    """
+    if not os.path.isfile(path):
+        raise FileNotFoundError(f"index file not found: {path}")
+    with open(path, "rb") as f:
+        if f.read(8) != _MAGIC:
+            raise ValueError(f"not a rotormap index container: {path}")
+        hl = int(np.frombuffer(f.read(8), np.uint64)[0])
+        meta = json.loads(f.read(hl))
+    base = (len(_MAGIC) + 8 + hl + 63) // 64 * 64
+    if meta.get("format") not in (FP8_FORMAT, SCALED_FORMAT):
+        raise ValueError(f"not an {FP8_FORMAT} index: {path}")
+    if meta["normalize"] != 0:
+        raise ValueError(f"mapping assumes a normalize = 0 index (got {meta['normalize']})")
+    arrs = {}
+    for name, d in meta["arrays"].items():
+        shape = tuple(d["shape"])
+        if mmap:
+            arrs[name] = np.memmap(path, dtype=np.dtype(d["dtype"]), mode="r", offset=base + d["offset"],
+                                   shape=shape) if int(np.prod(shape)) else np.zeros(shape, np.dtype(d["dtype"]))
+        else:
+            with open(path, "rb") as f:
+                f.seek(base + d["offset"])
+                arrs[name] = np.frombuffer(f.read(int(np.prod(shape)) * np.dtype(d["dtype"]).itemsize),
+                                           np.dtype(d["dtype"])).reshape(shape)
+    rdim = 2 * meta["m"] * 4 ** meta["c"]
+    N = 2 * meta["n_frag"]
+    if tuple(arrs["embeds8"].shape) != (N, rdim):
+        raise ValueError("embeds8 shape mismatch")
+    for nm in ("col_rec", "starts", "strand"):
+        if arrs[nm].shape[0] != N:
+            raise ValueError("meta length mismatch")
+    emb = arrs["embeds8"]
+    scales = arrs.get("scales")
+    if device is not None:
+        emb = torch.from_numpy(np.ascontiguousarray(emb)).to(device)
+        if scales is not None:
+            scales = torch.from_numpy(np.ascontiguousarray(scales)).to(device)
+    return Index(format=meta["format"], source=meta["source"], k=meta["k"], kstep=meta["kstep"],
+                 s=meta["s"], m=meta["m"], c=meta["c"], normalize=meta["normalize"],
+                 n_frag=meta["n_frag"], embeds8=emb, norms=arrs["norms"], rec_heads=meta["rec_heads"],
+                 col_rec=arrs["col_rec"], starts=arrs["starts"], strand=arrs["strand"],
+                 col_pos=arrs["col_pos"], genome=arrs["genome"], rec_word_off=arrs["rec_word_off"],
+                 rec_nbases=arrs["rec_nbases"], batch_size=meta.get("batch_size", 8192),
+                 scales=scales)
+
+
+def index_database(idx: Index, device=None) -> torch.Tensor:
+    """index_database (load.jl:156-161): the resident e4m3 database B on the GPU."""
+    if isinstance(idx.embeds8, torch.Tensor) and idx.embeds8.is_cuda:
+        return idx.embeds8
+    dev = device if device is not None else "cuda"
+    return torch.from_numpy(np.ascontiguousarray(idx.embeds8)).to(dev)

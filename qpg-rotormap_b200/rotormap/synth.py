@@ -1,0 +1,162 @@
+"""Seeded synthetic genomes and reads (stand-ins for the reference's fixture
+generators in RotorMap/common/dna.jl and RotorMap/reads/sample.jl).
+
+The reference draws its fixtures from Julia's Xoshiro stream, which is not
+reproducible here; these generators keep the same shapes and models with
+numpy's PCG64:
+  * genome: iid bases with a GC fraction, optional N runs (lengths uniform
+    in [run_min, run_max]) covering a given fraction of the bases;
+  * `:even` read sampling over each record's N-free windows, midpoints of
+    equal strata with largest-remainder allocation (sample.jl:474-610);
+  * mutation: iid substitutions at rate `err` (each substituted base takes
+    one of the three other bases uniformly), or the reference's `mutate`
+    model (ceil(n*err) edits, 1/3 sub / ins / del, length kept).
+Headers follow the reference's provenance format
+`>read_<i> start=<1-based> len=<k> src=<record name>` (sample.jl:469-470).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+LETTERS = np.frombuffer(b"ACGT", np.uint8)
+
+
+def random_genome(lengths, seed: int = 1, gc: float = 0.5, n_frac: float = 0.0,
+                  run_min: int = 100, run_max: int = 10_000):
+    """Records as (codes uint8 0..3, nmask bool) pairs; N positions carry code 2
+    (G, the reference's code for any non-ACGT byte) and nmask True."""
+    rng = np.random.default_rng(seed)
+    p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
+    recs = []
+    for L in lengths:
+        codes = rng.choice(4, size=int(L), p=p).astype(np.uint8)
+        nmask = np.zeros(int(L), bool)
+        if n_frac > 0:
+            target = int(n_frac * L)
+            covered = 0
+            while covered < target:
+                ln = int(rng.integers(run_min, run_max + 1))
+                st = int(rng.integers(0, max(1, L - ln)))
+                seg = nmask[st:st + ln]
+                covered += int((~seg).sum())
+                nmask[st:st + ln] = True
+            codes[nmask] = 2
+        recs.append((codes, nmask))
+    return recs
+
+
+def genome_fasta(heads, recs, width: int = 70) -> bytes:
+    """FASTA text of the records (N runs written as 'N')."""
+    out = []
+    for h, (codes, nmask) in zip(heads, recs):
+        s = LETTERS[codes].copy()
+        s[nmask] = ord("N")
+        out.append(h.encode() + b"\n")
+        b = s.tobytes()
+        out.extend(b[i:i + width] + b"\n" for i in range(0, len(b), width))
+    return b"".join(out)
+
+
+def _nfree_window_starts(nmask: np.ndarray, k: int) -> np.ndarray:
+    """0-based starts of k-windows free of N (sample.jl `nfree` pool)."""
+    L = nmask.size
+    if L < k:
+        return np.zeros(0, np.int64)
+    c = np.concatenate([[0], np.cumsum(nmask.astype(np.int64))])
+    bad = c[k:] - c[:-k]
+    return np.flatnonzero(bad == 0).astype(np.int64)
+
+
+def even_alloc(w, n: int):
+    """_even_alloc (sample.jl:474-485): largest-remainder allocation."""
+    w = np.asarray(w, np.float64)
+    quota = n * w / w.sum()
+    alloc = np.floor(quota).astype(np.int64)
+    fr = quota - alloc
+    order = sorted(range(len(w)), key=lambda j: (-fr[j], j))
+    for t in range(n - int(alloc.sum())):
+        alloc[order[t]] += 1
+    return alloc
+
+
+def substitute(codes: np.ndarray, err: float, rng) -> np.ndarray:
+    """iid substitutions: each base is replaced with probability err by one of
+    the other three bases."""
+    out = codes.copy()
+    if err <= 0:
+        return out
+    hit = rng.random(out.size) < err
+    shift = rng.integers(1, 4, size=out.size).astype(np.uint8)
+    out[hit] = (out[hit] + shift[hit]) % 4
+    return out
+
+
+def mutate_edits(codes: np.ndarray, err: float, rng) -> np.ndarray:
+    """The reference's mutate model (dna.jl:120-183): ceil(n*err) edit
+    operations, 1/3 substitutions, 1/3 insertions, 1/3 deletions, the result
+    trimmed / padded back to the original length."""
+    n = codes.size
+    nops = math.ceil(n * err)
+    seq = list(codes.tolist())
+    for _ in range(nops):
+        op = int(rng.integers(0, 3))
+        if op == 0 and seq:
+            i = int(rng.integers(0, len(seq)))
+            seq[i] = (seq[i] + int(rng.integers(1, 4))) % 4
+        elif op == 1:
+            i = int(rng.integers(0, len(seq) + 1))
+            seq.insert(i, int(rng.integers(0, 4)))
+        elif seq:
+            i = int(rng.integers(0, len(seq)))
+            del seq[i]
+    while len(seq) < n:
+        seq.append(int(rng.integers(0, 4)))
+    return np.array(seq[:n], np.uint8)
+
+
+def sample_reads_even(heads, recs, n: int, k: int, err: float = 0.0, seed: int = 42,
+                      model: str = "subs"):
+    """`:even` draw over the N-free pool (sample.jl:566-582) -> (reads codes
+    list, provenance headers, record index, 1-based starts)."""
+    pools = [_nfree_window_starts(nm, k) for _, nm in recs]
+    w = np.array([p.size for p in pools], np.int64)
+    if w.sum() == 0:
+        raise ValueError(f"no N-free k = {k} window")
+    alloc = even_alloc(w, n)
+    rng = np.random.default_rng(seed)
+    reads, hd, rix, starts = [], [], [], []
+    i = 0
+    for j, nj in enumerate(alloc):
+        Wj = int(w[j])
+        for t in range(1, int(nj) + 1):
+            rank = 1 + ((2 * t - 1) * Wj) // (2 * nj) if nj <= Wj else ((t - 1) % Wj) + 1
+            st0 = int(pools[j][rank - 1])
+            codes = recs[j][0][st0:st0 + k]
+            if model == "subs":
+                codes = substitute(codes, err, rng)
+            else:
+                codes = mutate_edits(codes, err, rng)
+            i += 1
+            name = heads[j].split()[0][1:]
+            reads.append(codes)
+            hd.append(f">read_{i} start={st0 + 1} len={k} src={name}")
+            rix.append(j)
+            starts.append(st0 + 1)
+    return reads, hd, np.array(rix), np.array(starts)
+
+
+def reads_fasta(heads, reads) -> bytes:
+    return b"".join(h.encode() + b"\n" + LETTERS[r].tobytes() + b"\n" for h, r in zip(heads, reads))
+
+
+def pack_reads(reads, k: int) -> np.ndarray:
+    """Forward 2-bit words (n, cld(k,16)) of equal-length code arrays."""
+    n = len(reads)
+    W = (k + 15) // 16
+    codes = np.zeros((n, W * 16), np.uint32)
+    for i, r in enumerate(reads):
+        codes[i, :k] = r[:k]
+    sh = (2 * np.arange(16, dtype=np.uint32))[None, None, :]
+    return np.bitwise_or.reduce(codes.reshape(n, W, 16) << sh, axis=2).astype(np.uint32)

@@ -1,0 +1,142 @@
+"""GPU parity of the fused fp8 GEMM + top-k engine against the oracle's
+brute-force scores (the reference's checks: test_seg_rowtopk_merge_kernel,
+RotorMap/gemm/topk_kernels.jl:518-552, and _check_engine_gemm_topk,
+RotorMap/search/engine_fp8.jl:777-834)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as orc
+
+import rotormap as rm
+
+pytestmark = pytest.mark.gpu
+
+E4M3_INT = {0: 0x00, 1: 0x38, 2: 0x40, 3: 0x44, -1: 0xB8, -2: 0xC0, -3: 0xC4}
+
+
+def int_e4m3(rng, shape, lo=-3, hi=3):
+    """e4m3 bytes of small integers: every dot product is an exact small
+    integer in any summation order, so scores, ties and tie order are exact."""
+    v = rng.integers(lo, hi + 1, size=shape)
+    lut = np.zeros(7, np.uint8)
+    for x, b in E4M3_INT.items():
+        lut[x + 3] = b
+    return lut[v + 3], v
+
+
+def unit_e4m3(rng, n, rdim):
+    x = rng.standard_normal((n, rdim)).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    return orc.quantize_parity(x)
+
+
+def run_engine(A8, B8, k, score="f16", scaleA=None, scaleB=None, splits=0, ctas=0):
+    B = torch.from_numpy(B8).cuda()
+    A = torch.from_numpy(A8).cuda()
+    sb = torch.from_numpy(scaleB).cuda() if scaleB is not None else None
+    sa = torch.from_numpy(scaleA).cuda() if scaleA is not None else None
+    eng = rm.TopKEngine(B, k=k, rows_cap=A8.shape[0], score=score, scaleB=sb, splits=splits, ctas=ctas)
+    v, l = eng.search(A, A8.shape[0], sa)
+    torch.cuda.synchronize()
+    from rotormap._lib import check, lib
+    check(lib().r2m_check_device_error(None))
+    eng.close()
+    return v.cpu().numpy(), l.cpu().numpy()
+
+
+# the reference's top-k unit-test shapes (M, N) plus tile-edge cases
+SHAPES = [(64, 100), (257, 128), (1000, 333), (1, 4096), (511, 2048), (2048, 16384), (33, 37),
+          (64, 25), (64, 20), (129, 257), (128, 256), (300, 70001)]
+
+
+@pytest.mark.parametrize("nb,N", SHAPES)
+@pytest.mark.parametrize("score", ["f16", "f32"])
+def test_topk_exact_integer_scores(nb, N, score):
+    rng = np.random.default_rng(nb * 7 + N)
+    rdim = 256
+    A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
+    B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
+    k = 20
+    v, l = run_engine(A8, B8, k, score)
+    ov, ol = orc.topk_e4m3(A8, B8, k, 0 if score == "f16" else 1)
+    assert np.array_equal(v, ov)
+    assert np.array_equal(l, ol)  # ties broken by ascending column, exactly
+
+
+@pytest.mark.parametrize("k", [1, 5, 8, 16, 20, 32, 64])
+def test_topk_k_values(k):
+    rng = np.random.default_rng(k)
+    A8, _ = int_e4m3(rng, (200, 128))
+    B8, _ = int_e4m3(rng, (5000, 128))
+    v, l = run_engine(A8, B8, k)
+    ov, ol = orc.topk_e4m3(A8, B8, k, 0)
+    assert np.array_equal(v, ov) and np.array_equal(l, ol)
+
+
+@pytest.mark.parametrize("splits,ctas", [(1, 1), (3, 2), (7, 5), (0, 3), (128, 0)])
+def test_topk_schedules(splits, ctas):
+    """Forced column splits / few CTAs: several work units per CTA reuse the
+    TMEM double buffer across units."""
+    rng = np.random.default_rng(splits + 10 * ctas)
+    A8, _ = int_e4m3(rng, (300, 256))
+    B8, _ = int_e4m3(rng, (9000, 256))
+    v, l = run_engine(A8, B8, 20, splits=splits, ctas=ctas)
+    ov, ol = orc.topk_e4m3(A8, B8, 20, 0)
+    assert np.array_equal(v, ov) and np.array_equal(l, ol)
+
+
+@pytest.mark.parametrize("rdim", [16, 48, 128, 384, 2048])
+def test_topk_rdim_tails(rdim):
+    rng = np.random.default_rng(rdim)
+    A8, _ = int_e4m3(rng, (100, rdim), -1, 1)
+    B8, _ = int_e4m3(rng, (3000, rdim), -1, 1)
+    v, l = run_engine(A8, B8, 20, "f32")
+    ov, ol = orc.topk_e4m3(A8, B8, 20, 1)
+    assert np.array_equal(v, ov) and np.array_equal(l, ol)
+
+
+@pytest.mark.parametrize("score", ["f16", "f32", "scaled"])
+def test_topk_realistic_values_within_tolerance(score):
+    """Unit-norm rows quantised like the reference: the device accumulates in
+    fp32 in its own order, so scores may differ from the exact oracle by fp32
+    rounding (and, for f16, by one fp16 step at a rounding boundary)."""
+    rng = np.random.default_rng(11)
+    nb, N, rdim, k = 400, 20000, 2048, 20
+    A8 = unit_e4m3(rng, nb, rdim)
+    B8 = unit_e4m3(rng, N, rdim)
+    sa = sb = None
+    if score == "scaled":
+        sa = rng.uniform(0.5, 2.0, nb).astype(np.float32)
+        sb = rng.uniform(0.5, 2.0, N).astype(np.float32)
+    mode = {"f16": 0, "f32": 1, "scaled": 2}[score]
+    v, l = run_engine(A8, B8, k, score, sa, sb)
+    ov, ol = orc.topk_e4m3(A8, B8, k, mode, sa, sb)
+    tol = 1e-3 if score == "f16" else 2e-5
+    assert np.all(np.diff(v, axis=1) <= 0)
+    np.testing.assert_allclose(v, ov, atol=tol, rtol=0)
+    # every returned location carries its value, and the sets agree up to ties
+    for r in range(0, nb, 37):
+        sc = orc.scores_e4m3(A8[r], B8, mode, sb)
+        if score == "scaled":
+            sc = sc * sa[r]
+        np.testing.assert_allclose(sc[l[r] - 1], v[r], atol=tol, rtol=0)
+        kth = ov[r, -1]
+        assert np.all(sc[l[r] - 1] >= kth - 2 * tol)
+        strict = set(np.flatnonzero(sc > kth + 2 * tol) + 1)
+        assert strict <= set(l[r])
+
+
+def test_engine_rejects_bad_arguments():
+    B = torch.zeros((100, 64), dtype=torch.uint8, device="cuda")
+    with pytest.raises(ValueError):
+        rm.TopKEngine(B, k=101)
+    with pytest.raises(rm.R2MError):
+        from rotormap._lib import Tuning, lib, check
+        import ctypes
+        h = ctypes.c_void_p()
+        check(lib().r2m_engine_create(B.data_ptr(), None, 60, 100, 20, 10, 0, None, ctypes.byref(h)))
+    eng = rm.TopKEngine(B, k=20, rows_cap=8)
+    A = torch.zeros((9, 64), dtype=torch.uint8, device="cuda")
+    with pytest.raises(ValueError):
+        eng.search(A)
