@@ -118,7 +118,8 @@ typedef struct r2m_engine r2m_engine;
 typedef struct {
   int splits;  /* column splits per read tile (k-split of the top-k) */
   int ctas;    /* persistent CTAs (default: SM count) */
-  int reserved[6];
+  int reserved[6]; /* reserved[0] = 1: record CUDA events around the kernels
+                      of every r2m_batch_gemm_topk (see r2m_engine_kernel_ms) */
 } r2m_tuning;
 
 /* Replaces TopKEngine(B; k, w, rows_cap, segs, engine, cout)
@@ -133,6 +134,11 @@ int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int rdim,
 int r2m_engine_destroy(r2m_engine *eng);
 /* Bytes of device workspace the engine holds. */
 int64_t r2m_engine_workspace_bytes(const r2m_engine *eng);
+/* Device time of the last r2m_batch_gemm_topk's GEMM+top-k kernel and of
+ * its split-merge kernel (engines created with tuning.reserved[0] = 1);
+ * waits for that call to finish.  No reference counterpart (the reference
+ * times whole chunks with _timed_gpu, RotorMap/common/util.jl:67). */
+int r2m_engine_kernel_ms(r2m_engine *eng, float *gemm_ms, float *merge_ms, int *splits);
 
 /* Replaces batch_gemm_topk! (RotorMap/search/engine_fp8.jl:399-437) with the
  * cuBLASLt GEMM (fp8_lt.jl:128-168) and seg_rowtopk_merge_kernel!

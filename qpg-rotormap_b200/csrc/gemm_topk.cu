@@ -566,6 +566,9 @@ struct r2m_engine {
   int *part_cols;
   size_t part_lists;  // capacity in lists (rows x splits)
   uint32_t *err;
+  bool timing;        // record events around the two kernels of each call
+  cudaEvent_t ev[3];
+  int last_splits;
 };
 
 extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int rdim, int64_t N, int k,
@@ -596,6 +599,17 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   e->score_mode = score_mode;
   e->ctas = (tune && tune->ctas > 0) ? tune->ctas : sm_count();
   e->forced_splits = (tune && tune->splits > 0) ? tune->splits : 0;
+  e->timing = tune && tune->reserved[0] != 0;
+  e->last_splits = 0;
+  if (e->timing) {
+    for (int i = 0; i < 3; ++i) {
+      cudaError_t ce = cudaEventCreate(&e->ev[i]);
+      if (ce != cudaSuccess) {
+        delete e;
+        return cuda_fail(ce, "cudaEventCreate");
+      }
+    }
+  }
   e->n_tiles = (int)((N + BN - 1) / BN);
   rc = make_map(&e->mapB, d_B, N, rdim, BN);
   if (rc) {
@@ -633,6 +647,8 @@ extern "C" int r2m_engine_destroy(r2m_engine *eng) {
   if (!eng) return R2M_OK;
   cudaFree(eng->part_vals);
   cudaFree(eng->part_cols);
+  if (eng->timing)
+    for (int i = 0; i < 3; ++i) cudaEventDestroy(eng->ev[i]);
   delete eng;
   return R2M_OK;
 }
@@ -670,6 +686,8 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   if ((size_t)g.splits * g.mpad > eng->part_lists) return fail(R2M_ESTATE, "engine workspace too small");
   long long units = (long long)g.num_m_tiles * g.splits;
   int ctas = (int)(units < eng->ctas ? units : eng->ctas);
+  eng->last_splits = g.splits;
+  if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[0], st));
   switch (eng->KT) {
     case 8: rc = launch_gemm<8>(mapA, eng->mapB, g, ctas, st); break;
     case 16: rc = launch_gemm<16>(mapA, eng->mapB, g, ctas, st); break;
@@ -678,10 +696,25 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
     default: rc = launch_gemm<64>(mapA, eng->mapB, g, ctas, st); break;
   }
   if (rc) return rc;
+  if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[1], st));
   const int warps = 8;
   k_merge_splits<<<(nb + warps - 1) / warps, 32 * warps, 0, st>>>(
       eng->part_vals, eng->part_cols, g.splits, g.mpad, eng->KT, nb, eng->k, eng->score_mode, d_scaleA,
       d_vals, d_locs);
   R2M_CUDA(cudaGetLastError());
+  if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[2], st));
+  return R2M_OK;
+}
+
+extern "C" int r2m_engine_kernel_ms(r2m_engine *eng, float *gemm_ms, float *merge_ms, int *splits) {
+  R2M_REQUIRE(eng != nullptr, "engine is null");
+  R2M_REQUIRE(eng->timing, "engine was created without kernel timing (tuning.reserved[0] = 1)");
+  R2M_CUDA(cudaEventSynchronize(eng->ev[2]));
+  float a = 0.f, b = 0.f;
+  R2M_CUDA(cudaEventElapsedTime(&a, eng->ev[0], eng->ev[1]));
+  R2M_CUDA(cudaEventElapsedTime(&b, eng->ev[1], eng->ev[2]));
+  if (gemm_ms) *gemm_ms = a;
+  if (merge_ms) *merge_ms = b;
+  if (splits) *splits = eng->last_splits;
   return R2M_OK;
 }

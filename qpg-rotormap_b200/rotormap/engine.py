@@ -50,7 +50,7 @@ class TopKEngine:
 
     def __init__(self, B: torch.Tensor, k: int = 20, w: int | None = None, rows_cap: int = 8192,
                  segs: int | None = None, score: str = "f16", scaleB: torch.Tensor | None = None,
-                 splits: int = 0, ctas: int = 0):
+                 splits: int = 0, ctas: int = 0, timing: bool = False):
         _lib.require_device()
         if B.dtype != torch.uint8 or B.dim() != 2 or not B.is_cuda or not B.is_contiguous():
             raise ValueError("B must be a contiguous (N, rdim) uint8 CUDA tensor")
@@ -67,10 +67,17 @@ class TopKEngine:
         self.a8 = torch.zeros((rows_cap, rdim), dtype=torch.uint8, device=B.device)
         self.scaleA = torch.ones((rows_cap,), dtype=torch.float32, device=B.device)
         tune = Tuning(splits, ctas)
+        tune.reserved[0] = 1 if timing else 0
         h = ctypes.c_void_p()
         check(lib().r2m_engine_create(ptr(B), ptr(scaleB), rdim, N, k, rows_cap, _MODES[score],
                                       ctypes.byref(tune), ctypes.byref(h)))
         self._h = h
+
+    def kernel_ms(self):
+        """(gemm_ms, merge_ms, splits) of the last search (timing engines only)."""
+        g, m, sp = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+        check(lib().r2m_engine_kernel_ms(self._h, ctypes.byref(g), ctypes.byref(m), ctypes.byref(sp)))
+        return g.value, m.value, sp.value
 
     @property
     def workspace_bytes(self) -> int:
@@ -130,6 +137,50 @@ def batch_gemm_topk(D_val: torch.Tensor, D_loc: torch.Tensor, eng: TopKEngine, n
     sa = scaleA if scaleA is not None else (eng.scaleA if eng.score == "scaled" else None)
     eng.search(A, nb, sa, D_val, D_loc, stream)
     return D_val, D_loc
+
+
+class Mapper:
+    """Batch mapping through the public API with host buffers: packed read
+    words (host) -> H2D -> fused encode -> fp8 GEMM + top-k -> D2H of the
+    (nb, k) results.  Pinned staging is allocated once for `rows_cap` reads."""
+
+    def __init__(self, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stream=None):
+        self.eng, self.re, self.normalize = eng, re, normalize
+        dev = eng.B.device
+        cap = eng.rows_cap
+        self.stream = stream or torch.cuda.Stream(dev)
+        self.h_words = torch.empty((cap, re.words), dtype=torch.int32, pin_memory=True)
+        self.h_vals = torch.empty((cap, eng.k), dtype=torch.float32, pin_memory=True)
+        self.h_locs = torch.empty((cap, eng.k), dtype=torch.int32, pin_memory=True)
+        self.d_words = torch.empty((cap, re.words), dtype=torch.int32, device=dev)
+        self.d_norms = torch.empty((cap, re.m), dtype=torch.float32, device=dev)
+        self.d_vals = torch.empty((cap, eng.k), dtype=torch.float32, device=dev)
+        self.d_locs = torch.empty((cap, eng.k), dtype=torch.int32, device=dev)
+
+    def h2d_bytes(self, nb: int) -> int:
+        return nb * self.re.words * 4
+
+    def d2h_bytes(self, nb: int) -> int:
+        return nb * self.eng.k * 8
+
+    def map_words(self, words: np.ndarray | None = None, nb: int | None = None):
+        """Map `nb` reads whose packed words are in `words` (or already in
+        self.h_words).  Returns host views (vals (nb, k), locs (nb, k))."""
+        if words is not None:
+            nb = words.shape[0]
+            self.h_words[:nb].numpy().view(np.uint32)[:] = words
+        eng, st = self.eng, self.stream
+        scaled = eng.score == "scaled"
+        with torch.cuda.stream(st):
+            self.d_words[:nb].copy_(self.h_words[:nb], non_blocking=True)
+            a8 = eng.a8[:nb]
+            sa = eng.scaleA[:nb] if scaled else None
+            encode_frag_real_batch(a8, self.d_norms[:nb], self.re, self.d_words[:nb], self.normalize, sa, st)
+            eng.search(a8, nb, sa, self.d_vals[:nb], self.d_locs[:nb], st)
+            self.h_vals[:nb].copy_(self.d_vals[:nb], non_blocking=True)
+            self.h_locs[:nb].copy_(self.d_locs[:nb], non_blocking=True)
+        st.synchronize()
+        return self.h_vals[:nb].numpy(), self.h_locs[:nb].numpy()
 
 
 # ------------------------------------------------------------------ flows

@@ -216,7 +216,7 @@ def build_index(re: RopeEncoder, source, kstep: int | None = None, batch_size: i
     norms = torch.empty((N, re.m), dtype=torch.float32, device=dev)
     scales = torch.empty((N,), dtype=torch.float32, device=dev) if scaled else None
     if nwin:
-        g = torch.from_numpy(pack.words).to(dev)
+        g = torch.from_numpy(pack.words.view(np.int32)).to(dev)
         p = torch.from_numpy(pos).to(dev)
         kind = _lib.OUT_E4M3_SCALED if scaled else _lib.OUT_E4M3
         check(lib().r2m_encode_ref_windows(ptr(B), kind, ptr(norms), ptr(scales), ptr(g), ptr(p), nwin,
