@@ -152,6 +152,27 @@ int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A,
                         const float *d_scaleA, int nb, float *d_vals,
                         int32_t *d_locs, r2m_stream_t stream);
 
+/* Allocation-free variant of r2m_batch_gemm_topk for callers that cannot
+ * allocate device memory when they search: a thread capturing a CUDA graph,
+ * a serving loop where cudaMalloc would synchronize the device, or a host
+ * whose memory pool already owns the free device memory.  No counterpart in
+ * the reference.  Takes the engine's arguments directly (B, scaleB, rdim, N,
+ * k, score_mode as r2m_engine_create; A, scaleA, nb, outputs as
+ * r2m_batch_gemm_topk) and calls no cudaMalloc/cudaFree: the split scratch
+ * is a 32 MiB array inside the library that every GPU loading the library
+ * holds until exit.  Limit: ceil(nb/128)*128 rows x the top-k list size
+ * (k rounded up to 8/16/20/32/64) x 8 bytes must fit 32 MiB (nb <= 209,664
+ * at k = 20); larger nb returns R2M_EINVAL.  The first call on a device looks
+ * up the array's address and should come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialized by the caller.  A device-side
+ * wait that gave up marks every output row with NaN values and location -1. */
+int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_scaleB,
+                                int rdim, int64_t N, const uint8_t *d_A,
+                                const float *d_scaleA, int nb, int k,
+                                int score_mode, float *d_vals,
+                                int32_t *d_locs, r2m_stream_t stream);
+
 /* ------------------------------------------------------------ host FASTA */
 
 typedef struct r2m_reads r2m_reads;

@@ -718,3 +718,131 @@ extern "C" int r2m_engine_kernel_ms(r2m_engine *eng, float *gemm_ms, float *merg
   if (splits) *splits = eng->last_splits;
   return R2M_OK;
 }
+
+// ------------------------------------------------------------------
+// Allocation-free search.
+//
+// Some callers cannot allocate device memory at the point where they map a
+// batch: a thread that is capturing a CUDA graph, a serving loop where a
+// cudaMalloc would synchronize the device and stall other streams, or a host
+// whose memory pool (CUDA.jl's, PyTorch's caching allocator) already owns the
+// free device memory, so a side allocation can fail.  This entry point needs
+// no engine: the per-split partial top-k lists live in the file-scope array
+// below, whose device address is looked up once per device with
+// cudaGetSymbolAddress.  Every GPU that loads this library holds the array
+// (kNoAllocScratchBytes) until the process exits.
+namespace r2m {
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ __align__(256) uint32_t g_noalloc_err;
+
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_ptr[64];
+static uint32_t *g_noalloc_err_ptr[64];
+
+// Device addresses of the scratch array and error word on the current device
+// (set up on the first call per device).
+static int noalloc_setup(unsigned char **scratch, uint32_t **err) {
+  int dev = 0;
+  R2M_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(R2M_ESTATE, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void *p = nullptr, *q = nullptr;
+    R2M_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    R2M_CUDA(cudaGetSymbolAddress(&q, g_noalloc_err));
+    g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+    g_noalloc_err_ptr[dev] = static_cast<uint32_t *>(q);
+  }
+  *scratch = g_noalloc_ptr[dev];
+  *err = g_noalloc_err_ptr[dev];
+  return R2M_OK;
+}
+
+// A bounded wait that gave up leaves partial lists unwritten: mark every
+// output row invalid (NaN values, location -1) so the caller sees it.
+__global__ void k_noalloc_poison(const uint32_t *err, float *vals, int *locs, long long count) {
+  if (*err == 0) return;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    vals[i] = __int_as_float(0x7fc00000);
+    locs[i] = -1;
+  }
+}
+
+}  // namespace r2m
+
+extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_scaleB, int rdim, int64_t N,
+                                           const uint8_t *d_A, const float *d_scaleA, int nb, int k,
+                                           int score_mode, float *d_vals, int32_t *d_locs,
+                                           r2m_stream_t stream) {
+  R2M_REQUIRE(d_B != nullptr, "B is null");
+  R2M_REQUIRE(rdim >= 16 && rdim % 16 == 0, "rdim must be a positive multiple of 16");
+  R2M_REQUIRE(N >= 1 && N <= (1LL << 31) - 1 - BN, "N out of range");
+  R2M_REQUIRE(k >= 1 && k <= 64 && k <= N, "need 1 <= k <= min(N, 64)");
+  R2M_REQUIRE(nb >= 0, "nb must be >= 0");
+  R2M_REQUIRE(score_mode >= R2M_SCORE_F16 && score_mode <= R2M_SCORE_SCALED, "bad score_mode");
+  if (nb == 0) return R2M_OK;
+  R2M_REQUIRE(d_A && d_vals && d_locs, "null pointer");
+  R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || (d_scaleA && d_scaleB), "scaled scores need scaleA and scaleB");
+  R2M_REQUIRE((reinterpret_cast<uintptr_t>(d_B) & 15) == 0 && (reinterpret_cast<uintptr_t>(d_A) & 15) == 0,
+              "A and B must be 16-byte aligned");
+  R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || (reinterpret_cast<uintptr_t>(d_scaleB) & 15) == 0,
+              "scaleB must be 16-byte aligned");
+  const int KT = pick_kt(k);
+  const int m_tiles = (nb + BM - 1) / BM;
+  const size_t list_bytes = (size_t)KT * (sizeof(float) + sizeof(int));
+  const size_t max_lists = kNoAllocScratchBytes / list_bytes;
+  if ((size_t)m_tiles * BM > max_lists)
+    return fail(R2M_EINVAL, "nb = " + std::to_string(nb) + " exceeds the allocation-free scratch (" +
+                                std::to_string(kNoAllocScratchBytes >> 20) + " MiB holds at most " +
+                                std::to_string(max_lists / BM * BM) + " rows at k = " + std::to_string(k) +
+                                "); split the batch or use r2m_batch_gemm_topk");
+  unsigned char *scratch = nullptr;
+  uint32_t *err = nullptr;
+  int rc = noalloc_setup(&scratch, &err);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  CUtensorMap mapA, mapB;
+  if ((rc = make_map(&mapB, d_B, N, rdim, BN))) return rc;
+  if ((rc = make_map(&mapA, d_A, nb, rdim, BM))) return rc;
+  const int n_tiles = (int)((N + BN - 1) / BN);
+  const int ctas_max = sm_count();
+  int splits = choose_splits(m_tiles, n_tiles, ctas_max, 0);
+  const int fit = (int)(max_lists / ((size_t)m_tiles * BM));
+  if (splits > fit) splits = fit;
+  GemmArgs g;
+  g.nb = nb;
+  g.num_m_tiles = m_tiles;
+  g.N = N;
+  g.n_tiles = n_tiles;
+  g.splits = splits;
+  g.num_kb = (rdim + BK - 1) / BK;
+  g.score_mode = score_mode;
+  g.mpad = m_tiles * BM;
+  g.scaleB = d_scaleB;
+  g.part_vals = reinterpret_cast<float *>(scratch);
+  g.part_cols = reinterpret_cast<int *>(scratch + (size_t)splits * g.mpad * KT * sizeof(float));
+  g.err = err;
+  // the error word must start at zero; the partial lists are fully
+  // rewritten by the kernel before the merge reads them
+  R2M_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+  long long units = (long long)m_tiles * splits;
+  int ctas = (int)(units < ctas_max ? units : ctas_max);
+  switch (KT) {
+    case 8: rc = launch_gemm<8>(mapA, mapB, g, ctas, st); break;
+    case 16: rc = launch_gemm<16>(mapA, mapB, g, ctas, st); break;
+    case 20: rc = launch_gemm<20>(mapA, mapB, g, ctas, st); break;
+    case 32: rc = launch_gemm<32>(mapA, mapB, g, ctas, st); break;
+    default: rc = launch_gemm<64>(mapA, mapB, g, ctas, st); break;
+  }
+  if (rc) return rc;
+  const int warps = 8;
+  k_merge_splits<<<(nb + warps - 1) / warps, 32 * warps, 0, st>>>(g.part_vals, g.part_cols, splits, g.mpad, KT,
+                                                                   nb, k, score_mode, d_scaleA, d_vals, d_locs);
+  R2M_CUDA(cudaGetLastError());
+  k_noalloc_poison<<<64, 256, 0, st>>>(err, d_vals, d_locs, (long long)nb * k);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}

@@ -53,6 +53,7 @@ SIGNATURES = [
     ("r2m_engine_kernel_ms", I, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
                                  ctypes.POINTER(I)]),
     ("r2m_batch_gemm_topk", I, [P, P, P, I, P, P, P]),
+    ("r2m_batch_gemm_topk_noalloc", I, [P, P, I, I64, P, P, I, I, I, P, P, P]),
     ("r2m_fasta_reads", I, [ctypes.c_char_p, SZ, I, I, ctypes.POINTER(P)]),
     ("r2m_reads_count", I64, [P]),
     ("r2m_reads_words", P, [P]),
