@@ -1,0 +1,194 @@
+"""CPU tests of the host side: the C ABI exports, the native FASTA reader
+against the oracle restatement of RotorMap/fasta/reader.jl, reference-window
+enumeration (RotorMap/index/build.jl:291-324), the index container, the
+map.jl table formatting and the provenance scorer.  No GPU is needed."""
+import re as _re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+import rotormap as rm
+from rotormap import _lib, synth
+from rotormap.index import Index, batch_column_order
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def header_symbols():
+    txt = (ROOT / "include" / "r2m.h").read_text()
+    txt = _re.sub(r"/\*.*?\*/", "", txt, flags=_re.S)
+    return sorted(set(_re.findall(r"\b(r2m_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    L = _lib.lib()
+    syms = header_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), f"{s} declared in r2m.h but not exported"
+    bound = {n for n, _, _ in _lib.SIGNATURES}
+    assert set(syms) == bound, "ctypes signatures and r2m.h disagree"
+    assert L.r2m_version() >= 10000
+
+
+def test_device_entry_points_fail_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(_lib.R2MError):
+        _lib.require_device()
+
+
+FASTA_CASES = [
+    b"",
+    b"no record here\nACGT\n",
+    b"junk line\n>r1 first\nACGTACGTAC\nGTACGTACGT\n>r2\nAC\n",
+    b">crlf\r\nACGTNNNNacgtRYK\r\nTTTT\r\n>x\r\nGGGGGGGGGGGGGGGGGGGGGG\r\n",
+    b">a\nAC>GT ACGT\nAAAAAAAAAAAAAAAAAAAAA\n>b\n\n\nCCCCCCCCCCCCCCCCCCCCCCCCCCC",
+    b">only header at eof",
+    b">h1\nACGTACGTACGTACGTACGTACGTACGTACGT\n>h2 no newline before next\r>h3\nAAAAAAAAAAAAAAAAAAAAAAAAAAA\n",
+    b">r\n" + b"ACGT" * 64 + b"\n>s\n" + b"T" * 31 + b"\n>t\n" + b"G" * 32 + b"\n>u\n" + b"C" * 33 + b"\n",
+]
+
+
+@pytest.mark.parametrize("k", [1, 5, 16, 17, 31, 32, 33, 150])
+@pytest.mark.parametrize("ci", range(len(FASTA_CASES)))
+def test_fasta_reader_matches_oracle(ci, k):
+    raw = FASTA_CASES[ci]
+    got = rm.fasta_reads(raw, k=k, parts=1)
+    ref = orc.fasta_reads_ref(raw, k)
+    assert got.heads == [h for h, _ in ref]
+    if ref:
+        assert np.array_equal(got.words, np.stack([w for _, w in ref]))
+    else:
+        assert got.words.shape[0] == 0
+
+
+def test_fasta_reader_threads_do_not_change_the_result():
+    recs = synth.random_genome([1000] * 6000, seed=9)
+    heads = [f">rec_{i} x" for i in range(6000)]
+    raw = synth.genome_fasta(heads, recs, width=60)
+    assert len(raw) > (1 << 22)
+    a = rm.fasta_reads(raw, k=150, parts=1)
+    b = rm.fasta_reads(raw, k=150, parts=8)
+    assert a.heads == b.heads == heads
+    assert np.array_equal(a.words, b.words)
+    ref = orc.fasta_reads_ref(raw[:20000], 150)
+    assert [h for h, _ in ref] == a.heads[:len(ref)]
+    assert np.array_equal(np.stack([w for _, w in ref]), a.words[:len(ref)])
+
+
+def test_reference_windows_match_oracle():
+    recs = synth.random_genome([700, 149, 150, 333, 2000], seed=4, n_frac=0.1, run_min=5, run_max=40)
+    heads = [">A one", ">B", ">C", ">D", ">E"]
+    fa = b"leading junk\n" + synth.genome_fasta(heads, recs, width=37).replace(b"T", b"t", 50)
+    for k, kstep in ((150, 15), (150, 150), (50, 1), (17, 3)):
+        pack = rm.pack_reference(fa)
+        pos, rec, st = rm.window_positions(pack, k, kstep)
+        ref = orc.ref_windows_ref(fa, k, kstep)
+        assert len(ref) == pos.size
+        W = (k + 15) // 16
+        for i, (hd, start, words) in enumerate(ref):
+            assert pack.heads[rec[i]] == hd and st[i] == start
+            p = int(pos[i])
+            q, sh = p >> 4, 2 * (p & 15)
+            g = pack.words.astype(np.uint64)
+            for j in range(W):
+                v = (int(g[q + j]) >> sh) | ((int(g[q + j + 1]) << (32 - sh)) & 0xFFFFFFFF if sh else 0)
+                v &= 0xFFFFFFFF
+                if j == W - 1 and k & 15:
+                    v &= (1 << (2 * (k & 15))) - 1
+                assert v == int(words[j])
+
+
+def test_batch_column_layout():
+    col_win, strand = batch_column_order(10, 4)
+    assert list(col_win) == [0, 1, 2, 3, 0, 1, 2, 3, 4, 5, 6, 7, 4, 5, 6, 7, 8, 9, 8, 9]
+    assert list(strand) == [0] * 4 + [1] * 4 + [0] * 4 + [1] * 4 + [0, 0, 1, 1]
+
+
+def test_index_container_round_trip(tmp_path):
+    rng = np.random.default_rng(2)
+    N, rdim, m = 40, 64, 2  # rdim = 2*m*4^c with c = 2
+    pack = rm.pack_records([">r1 a", ">r2"], [rng.integers(0, 4, 300, dtype=np.uint8),
+                                             rng.integers(0, 4, 100, dtype=np.uint8)])
+    idx = Index(format=rm.FP8_FORMAT, source="x.fa", k=20, kstep=2, s=5, m=m, c=2, normalize=0, n_frag=N // 2,
+                embeds8=rng.integers(0, 256, (N, rdim), dtype=np.uint8),
+                norms=rng.random((N, m), dtype=np.float32), rec_heads=pack.heads,
+                col_rec=rng.integers(0, 2, N).astype(np.int32), starts=rng.integers(1, 99, N),
+                strand=(np.arange(N) % 2).astype(np.uint8), col_pos=rng.integers(0, 999, N),
+                genome=pack.words, rec_word_off=pack.word_off, rec_nbases=pack.nbases)
+    p = tmp_path / "t.r2mi"
+    idx.save(p)
+    back = rm.load_index(str(p))
+    for name in ("embeds8", "norms", "col_rec", "starts", "strand", "col_pos", "genome"):
+        assert np.array_equal(np.asarray(getattr(back, name)), np.asarray(getattr(idx, name))), name
+    assert back.rec_heads == idx.rec_heads and back.k == 20 and back.heads[0] == idx.heads[0]
+    with pytest.raises(ValueError):
+        bad = tmp_path / "bad.bin"
+        bad.write_bytes(b"not an index at all")
+        rm.load_index(str(bad))
+
+
+@pytest.mark.parametrize("x,s", [(0.9873047, "0.9873047"), (1.0, "1.0"), (0.5, "0.5"), (-0.25, "-0.25"),
+                                 (1e-5, "1.0e-5"), (0.0001, "0.0001"), (3.1415e-5, "3.1415e-5"),
+                                 (123456.0, "123456.0"), (1e6, "1.0e6"), (0.1, "0.1"), (-1e-7, "-1.0e-7"),
+                                 (0.0, "0.0"), (float("-inf"), "-Inf"), (0.0012345, "0.0012345"),
+                                 (1.2345678e8, "1.2345678e8")])
+def test_julia_float32_repr(x, s):
+    assert rm.julia_repr_f32(x) == s
+
+
+def test_parse_read_head_formats():
+    h = rm.parse_read_head(">read_12 start=345 len=150 src=chrA extra words")
+    assert h == dict(id=">read_12", start=345, len=150, src="chrA extra words")  # id keeps the ">"
+    h = rm.parse_read_head(">NC_000001.11:80433546:false")
+    assert h["start"] == 80433547 and h["len"] is None and h["src"] == "NC_000001.11"
+    assert rm.parse_read_head(">NC_11:49059499:true#2")["start"] == 49059500
+    for bad in ("read_1 start=1 len=2 src=a", ">read_1 start=x len=2 src=a", ">read_1 len=2 src=a",
+                ">a:b:true", ">a:1:maybe", ">a:1", ">read_1 start=1 len=2"):
+        assert rm.parse_read_head(bad) is None
+    for h in (">read_3 start=10 len=150 src=chrB", ">chrQ:99:true"):
+        assert rm.parse_read_head(h) == orc.parse_read_head(h)
+
+
+def test_provenance_scoring_matches_oracle():
+    rng = np.random.default_rng(5)
+    k, N, ktop = 150, 600, 20
+    rec_heads = [">chrA one", ">chrB"]
+    col_rec = rng.integers(0, 2, N).astype(np.int32)
+    starts = rng.integers(1, 5000, N)
+    idx = Index(format=rm.FP8_FORMAT, source="", k=k, kstep=15, s=8, m=4, c=4, normalize=0, n_frag=N // 2,
+                embeds8=np.zeros((N, 16), np.uint8), norms=np.zeros((N, 4), np.float32), rec_heads=rec_heads,
+                col_rec=col_rec, starts=starts, strand=np.zeros(N, np.uint8), col_pos=np.zeros(N, np.int64),
+                genome=np.zeros(1, np.uint32), rec_word_off=np.zeros(2, np.int64), rec_nbases=np.zeros(2, np.int64))
+    heads, locs = [], []
+    for i in range(300):
+        src = "chrA" if i % 2 else "chrB"
+        heads.append(f">read_{i} start={int(rng.integers(1, 5000))} len={k} src={src}")
+        locs.append(rng.choice(N, ktop, replace=False) + 1)
+    locs = np.array(locs)
+    got = rm.score_provenance(heads, locs, idx, ktop)
+    ref = orc.map_and_count_ref(heads, locs, idx.heads, list(starts), k, ktop)
+    assert got[0] == ref[0] and got[1] == ref[1] and list(got[2]) == ref[2]
+    assert got[3] == ref[3] and got[4] == ref[4]
+
+
+def test_synth_even_sampler_and_packing():
+    heads = [">g1 a", ">g2 b"]
+    recs = synth.random_genome([5000, 3000], seed=1, gc=0.41, n_frac=0.05, run_min=20, run_max=100)
+    reads, hd, rix, st = synth.sample_reads_even(heads, recs, 200, 150, 0.0, seed=3)
+    assert len(reads) == 200 and list(synth.even_alloc([3, 1], 4)) == [3, 1]
+    for r, h, j, s0 in zip(reads, hd, rix, st):
+        codes, nmask = recs[j]
+        assert not nmask[s0 - 1:s0 - 1 + 150].any()
+        assert np.array_equal(r, codes[s0 - 1:s0 - 1 + 150])
+        assert rm.parse_read_head(h)["start"] == s0
+    w = synth.pack_reads(reads[:5], 150)
+    for i in range(5):
+        assert np.array_equal(w[i], orc.forward_pack(reads[i], 150))
+    mutated = synth.substitute(np.zeros(100000, np.uint8), 0.05, np.random.default_rng(0))
+    assert abs((mutated != 0).mean() - 0.05) < 0.005

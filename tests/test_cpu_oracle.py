@@ -1,0 +1,117 @@
+"""CPU checks of the oracle itself: golden vectors, published encodings and
+the reference's own known-answer properties.  No GPU is needed."""
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import random_words
+from oracle import oracle as orc
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "rope_golden.json").read_text())
+CODE = {"A": 0, "C": 1, "G": 2, "T": 3}
+
+
+def golden_words(case):
+    codes = np.array([CODE[case["unit"][j % len(case["unit"])]] for j in range(case["k"])], np.uint8)
+    return orc.forward_pack(codes, case["k"])[None, :]
+
+
+def golden_dense(case):
+    nbin = case["nbin"]
+    out = np.zeros(2 * nbin)
+    for b, (re, im) in case["bins"].items():
+        out[int(b)] = re
+        out[nbin + int(b)] = im
+    return out
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=[c["name"] for c in GOLDEN])
+def test_oracle_f64_matches_closed_form(case):
+    w = golden_words(case)
+    out, norms = orc.rope_f64(w, case["k"], case["s"], case["m"], case["c"], 0)
+    np.testing.assert_allclose(out[0], golden_dense(case), rtol=0, atol=1e-12)
+    assert math.isclose(norms[0, 0], case["norm"], rel_tol=1e-12)
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=[c["name"] for c in GOLDEN])
+def test_oracle_f32_matches_closed_form(case):
+    w = golden_words(case)
+    out, norms = orc.rope_f32(w, case["k"], case["s"], case["m"], case["c"], 0)
+    # periodic fragments pour ~nw/P windows into each bin: fp32 summation
+    # error grows with the window count
+    nw = case["k"] - case["s"] + 1
+    np.testing.assert_allclose(out[0], golden_dense(case), rtol=1e-5, atol=2e-6 * max(1.0, nw / 150))
+
+
+# OCP FP8 E4M3 (bias 7, max 448, NaN = S.1111.111, no Inf): value -> byte
+E4M3_KNOWN = [
+    (0.0, 0x00), (-0.0, 0x80), (1.0, 0x38), (-1.0, 0xB8), (1.5, 0x3C), (2.0, 0x40), (3.0, 0x44),
+    (448.0, 0x7E), (-448.0, 0xFE), (240.0, 0x77), (256.0, 0x78), (2.0 ** -6, 0x08),
+    (2.0 ** -9, 0x01), (7 * 2.0 ** -9, 0x07), (0.875, 0x36),
+    (1.0625, 0x38),     # tie between 1.0 and 1.125 -> even mantissa (1.0)
+    (1.1875, 0x3A),     # tie between 1.125 and 1.25 -> even (1.25)
+    (500.0, 0x7E), (1e9, 0x7E), (float("inf"), 0x7E), (-1e9, 0xFE),  # satfinite
+    (2.0 ** -11, 0x00), (2.0 ** -10, 0x00),  # below / at half the smallest subnormal
+    (3 * 2.0 ** -11, 0x01), (2.0 ** -10 * 1.0001, 0x01),
+    (464.0, 0x7E),      # tie 448/480 -> 480 overflows -> saturates
+]
+
+
+@pytest.mark.parametrize("x,b", E4M3_KNOWN)
+def test_e4m3_known_encodings(x, b):
+    assert orc.f32_to_e4m3(np.array([x], np.float32))[0] == b
+
+
+def test_e4m3_decode_table_and_round_trip():
+    t = orc.e4m3_table()
+    for b in range(256):
+        s, e, m = b >> 7, (b >> 3) & 15, b & 7
+        if e == 15 and m == 7:
+            assert math.isnan(t[b])
+            continue
+        v = (m / 8.0) * 2.0 ** -6 if e == 0 else (1 + m / 8.0) * 2.0 ** (e - 7)
+        assert t[b] == (-v if s else v)
+        assert orc.f32_to_e4m3(np.array([t[b]], np.float32))[0] == b
+
+
+def test_fp16_rounding_matches_ieee():
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.standard_normal(1 << 18) * s for s in (1e-7, 1e-5, 1e-3, 1, 1e3, 6e4)])
+    x = np.concatenate([x, [65504.0, 65519.0, 65520.0, 2.0 ** -24, 2.0 ** -25, 3 * 2.0 ** -26,
+                            2.0 ** -14, 2.0 ** -14 - 2.0 ** -25]]).astype(np.float32)
+    got = orc.f32_to_f16_bits(x)
+    ref = x.astype(np.float16).view(np.uint16)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("k,s,m,c", [(150, 8, 4, 4), (37, 5, 1, 3), (2001, 5, 1, 4), (20, 8, 2, 2)])
+def test_oracle_f32_tracks_f64_and_unit_energy(k, s, m, c):
+    rng = np.random.default_rng(k)
+    w = random_words(rng, 32, k)
+    o64, n64 = orc.rope_f64(w, k, s, m, c, 0)
+    o32, n32 = orc.rope_f32(w, k, s, m, c, 0)
+    np.testing.assert_allclose(o32, o64, rtol=1e-5, atol=2e-6)
+    np.testing.assert_allclose((o64 ** 2).sum(axis=1), 1.0, rtol=1e-12)
+    np.testing.assert_allclose(n32[:, 0], n64[:, 0], rtol=1e-5)
+
+
+def test_revcomp_reference_identities():
+    rng = np.random.default_rng(1)
+    for k in (1, 7, 16, 17, 150):
+        w = random_words(rng, 4, k)
+        for f in range(4):
+            rc = orc.revcomp_words_ref(w[f], k)
+            assert np.array_equal(orc.revcomp_words_ref(rc, k), w[f])
+            codes = orc.frag_codes(w[f], k)
+            assert np.array_equal(orc.frag_codes(rc, k), (3 - codes[::-1]).astype(np.uint8))
+
+
+def test_topk_oracle_orders_ties_by_column():
+    A = np.full((1, 16), 0x38, np.uint8)
+    B = np.zeros((10, 16), np.uint8)
+    B[[2, 5, 7]] = 0x38          # three columns tie at the top score
+    v, l = orc.topk_e4m3(A, B, 4, 1)
+    assert list(l[0]) == [3, 6, 8, 1] and list(v[0]) == [16.0, 16.0, 16.0, 0.0]
