@@ -209,6 +209,7 @@ def main():
     ap.add_argument("--ncols", type=int, default=N_COLS)
     ap.add_argument("--reads", type=int, default=Q)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--splits", type=int, default=0, help="force the column split count (0 = auto)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -242,7 +243,8 @@ def main():
     nq = words.shape[0]
     dev = torch.device("cuda", local)
     d_words = torch.from_numpy(words.reshape(-1).view(np.int32)).to(dev)
-    eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=nq, score="scaled", scaleB=idx.scales, timing=True)
+    eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=nq, score="scaled", scaleB=idx.scales, timing=True,
+                        splits=args.splits)
     a8, sa = eng.a8[:nq], eng.scaleA[:nq]
     norms = torch.empty((nq, M), dtype=torch.float32, device=dev)
     d_val = torch.empty((nq, TOPK), dtype=torch.float32, device=dev)

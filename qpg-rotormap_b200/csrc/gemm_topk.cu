@@ -66,15 +66,16 @@ __device__ __forceinline__ int split_lo(int s, int n_tiles, int splits) {
 
 __device__ __forceinline__ float round_f16(float x) { return __half2float(__float2half_rn(x)); }
 
-// Reservoir of the best KT (value, column) pairs; order: larger value first,
-// equal values -> smaller column first.  `thr`/`mc` track the worst entry.
+// The best KT (value, column) pairs of one row, kept sorted in registers:
+// larger value first, equal values -> smaller column first.  `thr` is the
+// worst kept value.  Insertion is branch-free: the new entry's rank is a sum
+// of independent compares and every slot picks (old, shifted, new) with two
+// selects, so there is no dependent chain through the list.
 template <int KT>
 struct Reservoir {
   float v[KT];
   int c[KT];
   float thr;
-  int mc;
-  int minpos;
 
   __device__ __forceinline__ void reset() {
 #pragma unroll
@@ -83,46 +84,26 @@ struct Reservoir {
       c[i] = INT_MAX;
     }
     thr = -INFINITY;
-    mc = INT_MAX;
-    minpos = 0;
   }
-  // Called only with x > thr: columns arrive in increasing order, so a tie
-  // with the worst entry never displaces it.
+  // Called only with x > thr and a column larger than every kept column (the
+  // scan runs in increasing column order), so the rank is #{v[i] >= x}.
   __device__ __forceinline__ void insert(float x, int col) {
+    int p = 0;
 #pragma unroll
-    for (int i = 0; i < KT; ++i)
-      if (i == minpos) {
-        v[i] = x;
-        c[i] = col;
-      }
-    float t = v[0];
-    int tc = c[0], tp = 0;
+    for (int i = 0; i < KT; ++i) p += (v[i] >= x) ? 1 : 0;
 #pragma unroll
-    for (int i = 1; i < KT; ++i) {
-      bool worse = (v[i] < t) || (v[i] == t && c[i] > tc);
-      t = worse ? v[i] : t;
-      tc = worse ? c[i] : tc;
-      tp = worse ? i : tp;
+    for (int i = KT - 1; i > 0; --i) {
+      const bool shift = i > p, here = i == p;
+      v[i] = shift ? v[i - 1] : (here ? x : v[i]);
+      c[i] = shift ? c[i - 1] : (here ? col : c[i]);
     }
-    thr = t;
-    mc = tc;
-    minpos = tp;
-  }
-  __device__ __forceinline__ void sort_desc() {
-#pragma unroll
-    for (int i = 0; i < KT; ++i) {
-#pragma unroll
-      for (int j = KT - 1; j > i; --j) {
-        bool swap = (v[j] > v[j - 1]) || (v[j] == v[j - 1] && c[j] < c[j - 1]);
-        float tv = swap ? v[j] : v[j - 1];
-        int tcol = swap ? c[j] : c[j - 1];
-        v[j] = swap ? v[j - 1] : v[j];
-        c[j] = swap ? c[j - 1] : c[j];
-        v[j - 1] = tv;
-        c[j - 1] = tcol;
-      }
+    if (p == 0) {
+      v[0] = x;
+      c[0] = col;
     }
+    thr = v[KT - 1];
   }
+  __device__ __forceinline__ void sort_desc() {}
 };
 
 template <int KT>
@@ -535,12 +516,8 @@ template <int KT>
 static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmArgs &g, int ctas,
                        cudaStream_t st) {
   size_t smem = gemm_smem_bytes();
-  static bool attr_set[8] = {false};
-  int slot = KT == 8 ? 0 : KT == 16 ? 1 : KT == 20 ? 2 : KT == 32 ? 3 : 4;
-  if (!attr_set[slot]) {
-    R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set[slot] = true;
-  }
+  // a function attribute is per device: set it on every launch (cheap)
+  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_gemm_topk<KT><<<ctas, THREADS, smem, st>>>(mA, mB, g);
   R2M_CUDA(cudaGetLastError());
   return R2M_OK;
