@@ -173,6 +173,27 @@ int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_scaleB,
                                 int score_mode, float *d_vals,
                                 int32_t *d_locs, r2m_stream_t stream);
 
+/* ------------------------------------------------------------ plain path */
+
+/* The reference engine's own structure on the B200 -- the plain batch path
+ * and the GPU bar of the fused kernel.  Replaces the same calls as
+ * r2m_engine_create / r2m_batch_gemm_topk (TopKEngine(B; engine = :lt,
+ * cout = :f16), RotorMap/search/engine_fp8.jl:309-437) but keeps their
+ * mechanics: a cuBLASLt fp8 GEMM (RotorMap/gemm/fp8_lt.jl:128-168) into
+ * double-buffered (rows x w) fp16 score chunks in HBM and the segmented top-k
+ * merge (RotorMap/gemm/topk_kernels.jl:213-347, segs = 8, k = 20) on a second
+ * stream.  d_A must hold ceil(nb/16)*16 rows (the pad rows are scored and
+ * dropped).  Outputs (nb, 20) row-major, 1-based ids, the reference's tie
+ * order. */
+typedef struct r2m_plain_engine r2m_plain_engine;
+int r2m_plain_engine_create(const uint8_t *d_B, int rdim, int64_t N, int k,
+                            int rows_cap, int w, int segs,
+                            r2m_plain_engine **out);
+int r2m_plain_engine_destroy(r2m_plain_engine *eng);
+int r2m_plain_batch_gemm_topk(r2m_plain_engine *eng, const uint8_t *d_A,
+                              int nb, float *d_vals, int32_t *d_locs,
+                              r2m_stream_t stream);
+
 /* ------------------------------------------------------------ host FASTA */
 
 typedef struct r2m_reads r2m_reads;

@@ -13,6 +13,9 @@ paths relative to the q4bio-qpg/qpg-rotormap tree):
                       RotorMap/common/harness.jl:52-91 (_e2h_ref_table)
   parse_read_head     RotorMap/reads/provenance.jl:46-78
   map_and_count_ref   RotorMap/search/engine_fp8.jl:654-733 (scoring loop)
+  seg_topk_merge_ref  RotorMap/gemm/topk_kernels.jl:213-329 (segmented top-k,
+                      its reservoir / merge tie rules)
+  batch_topk_ref      RotorMap/search/engine_fp8.jl:399-437 (chunk loop)
 C restatements (oracle/rotormap_oracle.c, built by oracle/Makefile):
   rope_f64 / rope_f32 / f32_to_e4m3 / f32_to_f16 / topk_e4m3 / scores_e4m3.
 
@@ -355,3 +358,62 @@ def map_and_count_ref(heads, locs, db_heads, db_starts, dbk: int, ktop: int):
                 inter_sum += ilen
                 inter_cnt += 1
     return total, correct, hist, inter_sum, inter_cnt
+
+
+def seg_topk_merge_ref(C: np.ndarray, offset: int, dv: np.ndarray, dl: np.ndarray, K: int = 20, PS: int = 8):
+    """One chunk of seg_rowtopk_merge_kernel! (RotorMap/gemm/topk_kernels.jl:213-329)
+    in plain Python: C (rows, wi) float32 scores of chunk columns offset+1..,
+    dv/dl (rows, K) the running lists (updated in place; ids 1-based)."""
+    rows, wi = C.shape
+    segw = -(-wi // PS)
+    for r in range(rows):
+        lists = []
+        for s in range(PS):
+            lo = s * segw
+            cnt = max(0, min(wi, (s + 1) * segw) - lo)
+            lk = [-np.inf] * K
+            li = [0] * K
+            thr, mp = -np.inf, 0
+            for c in range(cnt):
+                v = float(C[r, lo + c])
+                if v > thr:  # replace the tracked minimum
+                    lk[mp], li[mp] = v, c + 1
+                    mp = min(range(K), key=lambda j: (lk[j], j))  # first minimum
+                    thr = lk[mp]
+            for i in range(1, K):  # stable insertion sort, descending
+                v, d, j = lk[i], li[i], i
+                while j > 0 and lk[j - 1] < v:
+                    lk[j], li[j] = lk[j - 1], li[j - 1]
+                    j -= 1
+                lk[j], li[j] = v, d
+            lists.append((lk, li))
+        run_v, run_l = list(dv[r]), list(dl[r])
+        heads = [0] * PS
+        pa = 0
+        for j in range(K):
+            va = run_v[pa] if pa < K else -np.inf
+            bv, bs, bli = -np.inf, -1, 0
+            for s in range(PS):
+                h = heads[s]
+                if h < K and bv < lists[s][0][h]:  # ties keep the lowest segment
+                    bv, bs, bli = lists[s][0][h], s, lists[s][1][h]
+            if va >= bv:
+                dv[r, j] = va
+                dl[r, j] = run_l[pa] if pa < K else 0
+                pa += 1
+            else:
+                dv[r, j] = bv
+                dl[r, j] = 0 if bli == 0 else offset + bs * segw + bli
+                heads[bs] += 1
+    return dv, dl
+
+
+def batch_topk_ref(scores: np.ndarray, w: int, K: int = 20, PS: int = 8):
+    """batch_gemm_topk!'s chunk loop (RotorMap/search/engine_fp8.jl:399-437)
+    over a full (rows, N) score matrix."""
+    rows, N = scores.shape
+    dv = np.full((rows, K), -np.inf, np.float32)
+    dl = np.zeros((rows, K), np.int32)
+    for lo in range(0, N, w):
+        seg_topk_merge_ref(scores[:, lo:lo + w], lo, dv, dl, K, PS)
+    return dv, dl

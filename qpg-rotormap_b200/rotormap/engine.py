@@ -114,6 +114,53 @@ class TopKEngine:
         return D_val, D_loc
 
 
+class PlainEngine:
+    """The plain batch path: the reference engine's structure on the GPU
+    (cuBLASLt fp8 GEMM into fp16 chunks of `w` columns + segmented top-k,
+    engine_fp8.jl:290-437).  Same search() contract as TopKEngine for
+    score = "f16"; ties follow the reference's segment/reservoir order."""
+
+    def __init__(self, B: torch.Tensor, k: int = 20, w: int = 65536, rows_cap: int = 8192, segs: int = 8):
+        _lib.require_device()
+        if B.dtype != torch.uint8 or B.dim() != 2 or not B.is_cuda or not B.is_contiguous():
+            raise ValueError("B must be a contiguous (N, rdim) uint8 CUDA tensor")
+        self.B, self.k, self.N, self.rdim = B, k, B.shape[0], B.shape[1]
+        self.w = min(w, self.N)
+        self.rows_cap = (rows_cap + 15) // 16 * 16
+        self.score = "f16"
+        self.a8 = torch.zeros((self.rows_cap, self.rdim), dtype=torch.uint8, device=B.device)
+        h = ctypes.c_void_p()
+        check(lib().r2m_plain_engine_create(ptr(B), self.rdim, self.N, k, self.rows_cap, self.w, segs,
+                                            ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().r2m_plain_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, A8: torch.Tensor, nb: int | None = None, scaleA=None, D_val=None, D_loc=None,
+               stream=None):
+        """A8 must hold ceil(nb/16)*16 rows (use the engine's `a8` staging)."""
+        nb = A8.shape[0] if nb is None else nb
+        if nb > self.rows_cap or A8.shape[0] < (nb + 15) // 16 * 16:
+            raise ValueError("A8 must hold ceil(nb/16)*16 rows within rows_cap")
+        dev = self.B.device
+        if D_val is None:
+            D_val = torch.empty((nb, self.k), dtype=torch.float32, device=dev)
+        if D_loc is None:
+            D_loc = torch.empty((nb, self.k), dtype=torch.int32, device=dev)
+        check(lib().r2m_plain_batch_gemm_topk(self._h, ptr(A8), nb, ptr(D_val), ptr(D_loc),
+                                              stream_handle(stream)))
+        return D_val, D_loc
+
+
 def upload_fp16_as_f8(eng: TopKEngine, embeds, stream=None) -> torch.Tensor:
     """upload_fp16_as_f8! (engine_fp8.jl:355-371): H2D an fp16 (nb, rdim) batch
     and quantise it into the engine staging `a8` rows 0..nb-1."""
