@@ -197,6 +197,103 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- serving leg
+
+
+def serving_leg(dev, n_requests: int = 16, seed: int = 31):
+    """Serving form vs the plain batch path at human-scale geometry: 3.1 Gbp
+    genome of 24 records (lengths U[50, 250] Mbp rescaled, GC 41%, 5% N runs),
+    fwd + rc windows at k = 150, kstep = 1880 -> ~3.3M columns (~6.3 GiB e4m3),
+    Poisson arrivals of requests of U{1..100,000} reads with substitution
+    rates U[0, 0.10].  Same arrival schedule for every path."""
+    import torch
+    import rotormap as rm
+    from rotormap import serving, synth
+    re = rm.RopeEncoder(k=K_BASES, s=S, m=M, c=C)
+    lengths = synth.genome_lengths(3_100_000_000, 24, 50e6, 250e6, seed)
+    words, woff, nbases, runs = synth.random_genome_packed(lengths, seed=seed, gc=0.41, n_frac=0.05, device=dev)
+    heads = [f">chr{i + 1} synthetic human-scale record" for i in range(24)]
+    idx = rm.build_index_packed(re, words, heads, woff, nbases, 1880)
+    rng = np.random.default_rng(seed + 1)
+    sizes = rng.integers(1, 100_001, n_requests)
+    errs = rng.uniform(0.0, 0.10, n_requests)
+    reqs, truth = [], []
+    for i, n in enumerate(sizes):
+        recs, offs = synth.sample_positions(nbases, runs, int(n), K_BASES, seed + 10 + i)
+        reqs.append(synth.extract_reads_packed(words, woff, recs, offs, K_BASES, float(errs[i]), seed + 10 + i))
+        truth.append((recs, offs))
+    del words
+    torch.cuda.empty_cache()
+    total = int(sizes.sum())
+    # arrivals: Poisson, mean gap = mean request / (1.5 x a fused-kernel capacity estimate)
+    flop_per_read = 2.0 * re.rdim * idx.N
+    cap_est = 2.2e15 / flop_per_read
+    gaps = rng.exponential(float(sizes.mean()) / (1.5 * cap_est), n_requests)
+    arrivals = np.concatenate([[0.0], np.cumsum(gaps[1:])])
+
+    def replay(t0):
+        def wait(t):
+            d = t0 + t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+        return wait
+
+    def stats(done_times, t0):
+        lat = np.array([d - (t0 + a) for d, a in zip(done_times, arrivals)])
+        span = max(done_times) - t0
+        return {"reads_per_s": total / span, "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "span_s": span}
+
+    out = {"workload": f"3.1 Gbp genome (24 records, GC 41%, 5% N), k=150 kstep=1880 -> N={idx.N} "
+                       f"columns ({idx.N * re.rdim / 2**30:.2f} GiB e4m3), {n_requests} Poisson requests "
+                       f"of U{{1..100000}} reads (total {total}), subs U[0,0.10], top-20, f16 scores",
+           "index_cols": idx.N, "requests": n_requests, "reads": total}
+    # serving form (fused kernel, continuous batching)
+    eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=65536, score="f16")
+    srv = serving.MappingServer(eng, re)
+    srv.submit(reqs[0][:64]).result(300)  # warm-up
+    t0 = time.perf_counter()
+    wait = replay(t0)
+    hs = []
+    for a, w in zip(arrivals, reqs):
+        wait(a)
+        hs.append(srv.submit(w, t_arrival=t0 + a))
+    res = [h.result(600) for h in hs]
+    srv.close()
+    out["serving"] = stats([h.t_done for h in hs], t0)
+    out["serving"]["batches"] = srv.batches
+    out["serving"]["tflops"] = total * flop_per_read / out["serving"]["span_s"] / 1e12
+    # plain batch path, reference engine structure (cuBLASLt fp8 + segmented top-k, batch 8192)
+    peng = rm.PlainEngine(idx.embeds8, k=TOPK, w=65536, rows_cap=8192)
+    serving.plain_map(peng, re, [(0.0, reqs[0][:64])], batch=8192)
+    t0 = time.perf_counter()
+    pres = serving.plain_map(peng, re, list(zip(arrivals, reqs)), batch=8192, clock=replay(t0))
+    out["plain_reference_engine"] = stats([p[0] for p in pres], t0)
+    peng.close()
+    # plain batch path with the fused kernel (fixed 8192 batches, one request at a time)
+    t0 = time.perf_counter()
+    fres = serving.plain_map(eng, re, list(zip(arrivals, reqs)), batch=8192, clock=replay(t0))
+    out["plain_fused_kernel"] = stats([p[0] for p in fres], t0)
+    eng.close()
+    out["serving_vs_plain"] = out["serving"]["reads_per_s"] / out["plain_reference_engine"]["reads_per_s"]
+    # recall of the served top-20 against the reference-structured engine
+    ov, same = [], 0
+    for (v, l), (_, pv, pl) in zip(res, pres):
+        ov.append(np.mean([len(set(a) & set(b)) / TOPK for a, b in zip(l, pl)]))
+    out["top20_recall_vs_plain_reference"] = float(np.average(ov, weights=sizes))
+    # provenance: a read maps if a top-20 window overlaps its true position
+    hit = 0
+    recmap = idx.col_rec
+    for (v, l), (recs, offs) in zip(res, truth):
+        c = l.astype(np.int64) - 1
+        ok = (recmap[c] == recs[:, None]) & (np.abs(idx.starts[c] - (offs[:, None] + 1)) < K_BASES)
+        hit += int(ok.any(axis=1).sum())
+    out["mapped_frac_top20"] = hit / total
+    del idx
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- GPU leg
 
 
@@ -210,6 +307,8 @@ def main():
     ap.add_argument("--reads", type=int, default=Q)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--splits", type=int, default=0, help="force the column split count (0 = auto)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-vs-plain leg")
+    ap.add_argument("--requests", type=int, default=16, help="requests in the serving leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -338,8 +437,13 @@ def main():
         }
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(genome, words, os.cpu_count() or 1)
-        print(json.dumps(line), flush=True)
     eng.close()
+    del idx, eng, a8, sa, d_words, mapper
+    torch.cuda.empty_cache()
+    if rank == 0:
+        if world == 1 and not args.no_serving:
+            line["serving"] = serving_leg(dev, args.requests)
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

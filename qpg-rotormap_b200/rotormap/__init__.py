@@ -10,7 +10,8 @@ from .encoder import (RopeEncoder, dim, encode_frag_real_batch, encode_frag_real
 from .engine import (Mapper, PlainEngine, TopKBatch, TopKEngine, batch_gemm_topk, padmul, resident_fits,
                      rope_topk_stream, rope_topk_stream_compact, topk_flow, upload_fp16_as_f8)
 from .fasta import FastaFragments, fasta_reads
-from .index import (FP8_FORMAT, SCALED_FORMAT, Index, RefPack, build_index, index_database,
+from .index import (FP8_FORMAT, SCALED_FORMAT, Index, RefPack, build_index, build_index_packed,
+                    index_database,
                     load_index, pack_records, pack_reference, save_index, window_positions)
 from .mapping import julia_repr_f32, map_and_count, parse_read_head, run_map, score_provenance
 

@@ -234,6 +234,37 @@ def build_index(re: RopeEncoder, source, kstep: int | None = None, batch_size: i
                  scales=scales)
 
 
+def build_index_packed(re: RopeEncoder, words, rec_heads, rec_word_off, rec_nbases, kstep: int,
+                       batch_size: int = 8192, normalize: int = 0, scaled: bool = False,
+                       stream=None, source: str = "packed") -> Index:
+    """build_index over a genome that is already packed on the device
+    (int32/uint32 words, records on word boundaries with guard words)."""
+    _lib.require_device()
+    pack = RefPack(list(rec_heads), np.asarray(rec_word_off, np.int64), np.asarray(rec_nbases, np.int64),
+                   np.zeros(1, np.uint32))
+    pos, rec, st = window_positions(pack, re.k, kstep)
+    nwin = pos.size
+    col_win, strand = batch_column_order(nwin, batch_size)
+    dev = words.device
+    N = 2 * nwin
+    B = torch.empty((N, re.rdim), dtype=torch.uint8, device=dev)
+    norms = torch.empty((N, re.m), dtype=torch.float32, device=dev)
+    scales = torch.empty((N,), dtype=torch.float32, device=dev) if scaled else None
+    if nwin:
+        p = torch.from_numpy(pos).to(dev)
+        kind = _lib.OUT_E4M3_SCALED if scaled else _lib.OUT_E4M3
+        check(lib().r2m_encode_ref_windows(ptr(B), kind, ptr(norms), ptr(scales), ptr(words), ptr(p), nwin,
+                                           batch_size, re.k, re.s, re.m, re.c, normalize,
+                                           stream_handle(stream)))
+        torch.cuda.synchronize(dev)
+    return Index(format=SCALED_FORMAT if scaled else FP8_FORMAT, source=source, k=re.k, kstep=kstep,
+                 s=re.s, m=re.m, c=re.c, normalize=normalize, n_frag=nwin, embeds8=B,
+                 norms=norms.cpu().numpy(), rec_heads=list(rec_heads),
+                 col_rec=rec[col_win], starts=st[col_win], strand=strand, col_pos=pos[col_win],
+                 genome=np.zeros(1, np.uint32), rec_word_off=pack.word_off, rec_nbases=pack.nbases,
+                 batch_size=batch_size, scales=scales)
+
+
 # ------------------------------------------------------------------ file I/O
 
 _ARRAYS = ("embeds8", "norms", "col_rec", "starts", "strand", "col_pos", "genome", "rec_word_off",

@@ -160,3 +160,122 @@ def pack_reads(reads, k: int) -> np.ndarray:
         codes[i, :k] = r[:k]
     sh = (2 * np.arange(16, dtype=np.uint32))[None, None, :]
     return np.bitwise_or.reduce(codes.reshape(n, W, 16) << sh, axis=2).astype(np.uint32)
+
+
+# ------------------------------------------------------------------ on-device generators
+# Human-scale genomes (3.1 Gbp) are generated and packed on the GPU: numpy
+# would need minutes and ~12 GB of host memory for the same job.
+
+
+def genome_lengths(total: int, nrec: int, lo: float, hi: float, seed: int):
+    """Record lengths uniform on [lo, hi], rescaled to `total` bases."""
+    rng = np.random.default_rng(seed)
+    raw = rng.uniform(lo, hi, nrec)
+    L = np.floor(raw / raw.sum() * total).astype(np.int64)
+    L[-1] += total - L.sum()
+    return L
+
+
+def n_runs(length: int, frac: float, run_min: int, run_max: int, rng):
+    """Sorted, merged N runs [(start, end)) covering ~frac of a record."""
+    runs, covered = [], 0
+    target = int(frac * length)
+    while covered < target:
+        ln = int(rng.integers(run_min, run_max + 1))
+        st = int(rng.integers(0, max(1, length - ln)))
+        runs.append((st, st + ln))
+        covered += ln
+    runs.sort()
+    merged = []
+    for s, e in runs:
+        if merged and s <= merged[-1][1]:
+            merged[-1] = (merged[-1][0], max(merged[-1][1], e))
+        else:
+            merged.append((s, e))
+    return np.array(merged, np.int64).reshape(-1, 2)
+
+
+def random_genome_packed(lengths, seed: int = 1, gc: float = 0.5, n_frac: float = 0.0,
+                         run_min: int = 100, run_max: int = 10_000, device="cuda"):
+    """Records of iid bases (GC fraction `gc`, N runs coded as G like the
+    reference LUT) packed on the device: returns (words (int32 tensor, each
+    record starting on a word and followed by a zero guard word), word_off,
+    nbases, runs per record)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    chunks, offs, runs = [], [], []
+    cur = 0
+    sh = (2 * torch.arange(16, device=device, dtype=torch.int32)).view(1, 16)
+    p_a = (1 - gc) / 2
+    for L in lengths:
+        L = int(L)
+        nw = (L + 15) // 16
+        u = torch.rand(nw * 16, generator=gen, device=device)
+        codes = (u >= p_a).to(torch.int32) + (u >= 0.5).to(torch.int32) + (u >= 0.5 + gc / 2).to(torch.int32)
+        codes[L:] = 0
+        r = n_runs(L, n_frac, run_min, run_max, rng) if n_frac > 0 else np.zeros((0, 2), np.int64)
+        if r.size:
+            mark = torch.zeros(nw * 16 + 1, dtype=torch.int32, device=device)
+            mark.index_add_(0, torch.from_numpy(r[:, 0]).to(device), torch.ones(len(r), dtype=torch.int32, device=device))
+            mark.index_add_(0, torch.from_numpy(r[:, 1]).to(device), -torch.ones(len(r), dtype=torch.int32, device=device))
+            nmask = torch.cumsum(mark, 0)[:-1] > 0
+            codes[nmask] = 2
+            del mark, nmask
+        w = (codes.view(nw, 16) << sh).sum(dim=1, dtype=torch.int64).to(torch.int32)  # disjoint bits: sum == or
+        chunks += [w, torch.zeros(1, dtype=torch.int32, device=device)]
+        offs.append(cur)
+        cur += nw + 1
+        runs.append(r)
+        del u, codes
+    return torch.cat(chunks), np.array(offs, np.int64), np.asarray(lengths, np.int64), runs
+
+
+def sample_positions(nbases, runs, n: int, k: int, seed: int):
+    """n uniform read starts (record, 0-based offset) whose k-window avoids N runs."""
+    rng = np.random.default_rng(seed)
+    nb = np.asarray(nbases, np.int64)
+    w = np.maximum(nb - k + 1, 0).astype(np.float64)
+    recs, offs = [], []
+    while len(recs) < n:
+        m = n - len(recs)
+        r = rng.choice(len(nb), size=2 * m, p=w / w.sum())
+        o = (rng.random(2 * m) * w[r]).astype(np.int64)
+        for ri, oi in zip(r, o):
+            rr = runs[ri]
+            if rr.size:
+                j = np.searchsorted(rr[:, 0], oi + k)  # runs starting before the window end
+                if j > 0 and rr[j - 1, 1] > oi:
+                    continue
+            recs.append(int(ri))
+            offs.append(int(oi))
+            if len(recs) == n:
+                break
+    return np.array(recs), np.array(offs, np.int64)
+
+
+def extract_reads_packed(words, word_off, recs, offs, k: int, err, seed: int):
+    """Reads cut from the packed device genome at (record, offset), with iid
+    substitutions at per-read rates `err`, returned as packed (n, cld(k,16))
+    host words."""
+    import torch
+    dev = words.device
+    n = len(recs)
+    pos = torch.from_numpy(16 * np.asarray(word_off)[recs] + offs).to(dev)
+    j = torch.arange(k, device=dev)
+    p = pos[:, None] + j[None, :]
+    wv = words[(p >> 4)].to(torch.int64) & 0xFFFFFFFF
+    codes = ((wv >> (2 * (p & 15))) & 3).to(torch.int32)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    rate = torch.as_tensor(np.broadcast_to(np.asarray(err, np.float32), (n,)).copy(), device=dev)
+    hit = torch.rand((n, k), generator=gen, device=dev) < rate[:, None]
+    shift = torch.randint(1, 4, (n, k), generator=gen, device=dev, dtype=torch.int32)
+    codes = torch.where(hit, (codes + shift) % 4, codes)
+    W = (k + 15) // 16
+    pad = torch.zeros((n, W * 16), dtype=torch.int64, device=dev)
+    pad[:, :k] = codes
+    sh = (2 * torch.arange(16, device=dev, dtype=torch.int64)).view(1, 1, 16)
+    packed = (pad.view(n, W, 16) << sh).sum(dim=2)
+    return packed.to(torch.int64).cpu().numpy().astype(np.uint32)
