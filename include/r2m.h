@@ -173,6 +173,37 @@ int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_scaleB,
                                 int score_mode, float *d_vals,
                                 int32_t *d_locs, r2m_stream_t stream);
 
+/* ------------------------------------------------------- precision form */
+
+/* FP32 exact rescoring of top-k candidates.  No single reference
+ * counterpart: the reference scores only in fp8 (RotorMap/search/
+ * engine_fp8.jl:20-27) and checks against a CPU fp64 encode
+ * (_ref_rope_frag_real, RotorMap/encode/reference.jl:96-105).  For each of
+ * nb reads (forward words, as r2m_encode_frag_real_batch) and its kc <= 64
+ * candidate columns (1-based ids, e.g. an fp8 top-kc), re-encode the read and
+ * every candidate's reference window on the fly from the packed genome
+ * (genome / col_pos / strand as r2m_encode_ref_windows writes them; strand 1
+ * = reverse complement) in fp32 and score the unquantised embeddings' dot
+ * product.  scores (nb, kc) in candidate order (may be NULL); out_vals /
+ * out_locs (nb, topk) re-ranked, descending, ties by column. */
+int r2m_rescore_fp32(const uint32_t *dnas, int nb, const int32_t *cand, int kc,
+                     const uint32_t *genome, const int64_t *col_pos,
+                     const uint8_t *strand, int64_t N, int k, int s, int m,
+                     int c, int normalize, float *scores, float *out_vals,
+                     int32_t *out_locs, int topk, r2m_stream_t stream);
+
+/* FP64 sampled-row check: exact fp64 top-20 of S reads over all N index
+ * columns (re-encoded on the fly with the golden fp64 encoder semantics,
+ * RotorMap/encode/reference.jl:37-105, normalize = 0) -> d_vals / d_locs
+ * (S, 20), descending, ties by column; and, when d_cand is given, the fp64
+ * score of each (read, candidate) pair -> d_cand_scores (S, kc).  Allocates
+ * its own workspace; synchronizes the stream before returning. */
+int r2m_check_fp64(const uint32_t *d_read_words, int S, const uint32_t *d_genome,
+                   const int64_t *d_col_pos, const uint8_t *d_strand, int64_t N,
+                   int k, int s, int m, int c, const int32_t *d_cand, int kc,
+                   double *d_cand_scores, double *d_vals, int32_t *d_locs,
+                   r2m_stream_t stream);
+
 /* ------------------------------------------------------------ plain path */
 
 /* The reference engine's own structure on the B200 -- the plain batch path

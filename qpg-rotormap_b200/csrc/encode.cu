@@ -182,13 +182,13 @@ __device__ __forceinline__ float out_value(const EncParams &P, const float *hist
   return x;
 }
 
-// Encode the fragment whose words are staged in `words` (W words + a zero
-// guard word) with one warp; write row `row` (rdim elements of OUT), the m
-// norms and (scaled e4m3) the row scale.
-template <int OUT>
-__device__ void encode_fragment(const EncParams &P, const float2 *table, float *hist,
-                                uint16_t *cs, const uint32_t *words, float *nrmv, void *row,
-                                float *norms_out, float *scale_out) {
+// Histogram of the fragment whose words are staged in `words` (W words + a
+// zero guard word), built by one warp: phasor sums per bin in window order,
+// G-homopolymer bins zeroed, modes 2/3 reshaped; `nrmv` receives the divisor
+// of every copy (index 0 for mode 0) and `norms_out` the reference's norms
+// row.  The normalised value of split element i is hist[...]/nrmv[...].
+__device__ void fragment_hist(const EncParams &P, const float2 *table, float *hist, uint16_t *cs,
+                              const uint32_t *words, float *nrmv, float *norms_out) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
   // zero the histogram
@@ -289,6 +289,18 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
     }
   }
   __syncwarp();
+}
+
+// Encode the fragment whose words are staged in `words` (W words + a zero
+// guard word) with one warp; write row `row` (rdim elements of OUT), the m
+// norms and (scaled e4m3) the row scale.
+template <int OUT>
+__device__ void encode_fragment(const EncParams &P, const float2 *table, float *hist,
+                                uint16_t *cs, const uint32_t *words, float *nrmv, void *row,
+                                float *norms_out, float *scale_out) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+  fragment_hist(P, table, hist, cs, words, nrmv, norms_out);
   // output pass (amax first for the scaled form)
   float scale = 1.0f;
   if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
@@ -646,5 +658,160 @@ extern "C" int r2m_f16_to_e4m3(uint8_t *dst, const uint16_t *src, int64_t count,
   k_f16_to_e4m3<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(dst, reinterpret_cast<const __half *>(src),
                                                                   count);
   R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
+
+// ------------------------------------------------------------------
+// FP32 exact rescoring of top-k candidates.  For each read (one warp) the
+// fp32 embedding is rebuilt with the encoder's arithmetic, then every
+// candidate's reference window is re-encoded on the fly from the packed
+// genome (forward, or reverse complement for strand-1 columns) and scored as
+// the fp32 dot product of the two unquantised embeddings (fixed lane-strided
+// order + xor-tree reduction, so scores are deterministic).  The candidates
+// are re-ranked by that score (descending, ties by column).
+namespace r2m {
+
+constexpr int kMaxCand = 64;
+
+__global__ void __launch_bounds__(128) k_rescore_fp32(EncParams P, const uint32_t *__restrict__ dnas,
+                                                      int nb, const int *__restrict__ cand, int kc,
+                                                      const uint32_t *__restrict__ genome,
+                                                      const int64_t *__restrict__ col_pos,
+                                                      const uint8_t *__restrict__ strand, long long N,
+                                                      float *scores, float *out_v, int *out_l, int k,
+                                                      const float2 *gtable) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const float2 *table = block_table(P, smem, gtable);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+  unsigned char *base = smem + table_bytes(P);
+  const size_t per = warp_smem_bytes(P) + (size_t)P.rdim * 4 + 2 * kMaxCand * 4 + 32;
+  unsigned char *mine = base + per * warp;
+  WarpSmem ws = carve(P, mine, 0);
+  float *emb = reinterpret_cast<float *>(mine + warp_smem_bytes(P));
+  float *sc = emb + P.rdim;
+  int *scol = reinterpret_cast<int *>(sc + kMaxCand);
+  float *rnrm = reinterpret_cast<float *>(scol + kMaxCand);
+  const int nwarps_total = gridDim.x * (blockDim.x >> 5);
+  const int rstart = blockIdx.x * (blockDim.x >> 5) + warp;
+  const int W = P.W;
+  const int rr = P.k & 15;
+  const uint32_t tailmask = rr == 0 ? 0xFFFFFFFFu : ((1u << (2 * rr)) - 1u);
+  for (int row = rstart; row < nb; row += nwarps_total) {
+    // read embedding
+    for (int i = lane; i < W; i += 32) ws.words[i] = __ldg(dnas + (size_t)row * W + i);
+    if (lane == 0) ws.words[W] = 0u;
+    __syncwarp();
+    fragment_hist(P, table, ws.hist, ws.cs, ws.words, ws.nrmv, rnrm);
+    for (int i = lane; i < P.rdim; i += 32) emb[i] = out_value<R2M_OUT_F32>(P, ws.hist, ws.nrmv, i, 1.0f);
+    __syncwarp();
+    for (int j = 0; j < kc; ++j) {
+      const int c1 = __ldg(cand + (size_t)row * kc + j);
+      float s = -INFINITY;
+      if (c1 >= 1 && c1 <= N) {
+        const long long col = c1 - 1;
+        const int64_t pos = __ldg(col_pos + col);
+        const int64_t q = pos >> 4;
+        const uint32_t sh = (uint32_t)(pos & 15) << 1;
+        for (int t = lane; t < W; t += 32) {
+          uint32_t a = __ldg(genome + q + t), b = __ldg(genome + q + t + 1);
+          uint32_t v = sh == 0 ? a : ((a >> sh) | (b << (32u - sh)));
+          if (t == W - 1) v &= tailmask;
+          ws.words2[t] = v;
+        }
+        __syncwarp();
+        const uint32_t *src = ws.words2;
+        if (__ldg(strand + col)) {
+          for (int t = lane; t < W; t += 32) {
+            uint32_t w = 0;
+            for (int b = 0; b < 16; ++b) {
+              int x = 16 * t + b;
+              if (x < P.k) {
+                int y = P.k - 1 - x;
+                w |= (3u - ((ws.words2[y >> 4] >> (2 * (y & 15))) & 3u)) << (2 * b);
+              }
+            }
+            ws.words[t] = w;
+          }
+          src = ws.words;
+        }
+        if (lane == 0) {
+          ws.words[W] = 0u;
+          ws.words2[W] = 0u;
+        }
+        __syncwarp();
+        fragment_hist(P, table, ws.hist, ws.cs, src, ws.nrmv, rnrm);
+        float acc = 0.f;
+        for (int i = lane; i < P.rdim; i += 32)
+          acc = fmaf(emb[i], out_value<R2M_OUT_F32>(P, ws.hist, ws.nrmv, i, 1.0f), acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        s = acc;
+      }
+      if (lane == 0) {
+        sc[j] = s;
+        scol[j] = c1;
+        if (scores) scores[(size_t)row * kc + j] = s;
+      }
+      __syncwarp();
+    }
+    // re-rank (kc <= 64): lane 0 selection sort, value desc then column asc
+    if (lane == 0) {
+      for (int a = 0; a < k; ++a) {
+        int best = a;
+        for (int b = a + 1; b < kc; ++b) {
+          bool better = sc[b] > sc[best] || (sc[b] == sc[best] && scol[b] < scol[best]);
+          if (better) best = b;
+        }
+        float tv = sc[a];
+        int tc = scol[a];
+        sc[a] = sc[best];
+        scol[a] = scol[best];
+        sc[best] = tv;
+        scol[best] = tc;
+        out_v[(size_t)row * k + a] = sc[a];
+        out_l[(size_t)row * k + a] = sc[a] == -INFINITY ? 0 : scol[a];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace r2m
+
+extern "C" int r2m_rescore_fp32(const uint32_t *dnas, int nb, const int32_t *cand, int kc,
+                                const uint32_t *genome, const int64_t *col_pos, const uint8_t *strand,
+                                int64_t N, int k, int s, int m, int c, int normalize, float *scores,
+                                float *out_vals, int32_t *out_locs, int topk, r2m_stream_t stream) {
+  EncParams P;
+  int rc = make_params(P, k, s, m, c, normalize);
+  if (rc) return rc;
+  R2M_REQUIRE(nb >= 0, "nb must be >= 0");
+  R2M_REQUIRE(kc >= 1 && kc <= kMaxCand, "candidates per read must be in 1..64");
+  R2M_REQUIRE(topk >= 1 && topk <= kc, "need 1 <= topk <= candidates");
+  if (nb == 0) return R2M_OK;
+  R2M_REQUIRE(dnas && cand && genome && col_pos && strand && out_vals && out_locs, "null pointer");
+  cudaStream_t st = as_stream(stream);
+  size_t tb = ((size_t)P.m * P.nw * 8 + 15) & ~(size_t)15;
+  size_t per = warp_bytes_host(P) + (size_t)P.rdim * 4 + 2 * kMaxCand * 4 + 32;
+  P.table_in_smem = (tb + per * 4 <= 200 * 1024) ? 1 : 0;
+  size_t smem = (P.table_in_smem ? tb : 0) + per * 4;
+  R2M_REQUIRE(smem <= 220 * 1024, "rescoring shared memory does not fit (k or m*4^c too large)");
+  R2M_CUDA(cudaFuncSetAttribute(k_rescore_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  float2 *gt = nullptr;
+  if (!P.table_in_smem) {
+    R2M_CUDA(cudaMallocAsync(&gt, (size_t)P.m * P.nw * sizeof(float2), st));
+    int nchunk = (P.nw + P.Wc - 1) / P.Wc;
+    k_phasor_table<<<(nchunk * P.m + 127) / 128, 128, 0, st>>>(P, gt);
+  }
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rescore_fp32, 128, smem);
+  long long want = (nb + 3) / 4, cap = (long long)sm_count() * (per_sm > 0 ? per_sm : 1);
+  int grid = (int)(want < cap ? want : cap);
+  k_rescore_fp32<<<grid, 128, smem, st>>>(P, dnas, nb, cand, kc, genome, col_pos, strand, N, scores, out_vals,
+                                          out_locs, topk, gt);
+  cudaError_t e = cudaGetLastError();
+  if (gt) cudaFreeAsync(gt, st);
+  if (e != cudaSuccess) return cuda_fail(e, "k_rescore_fp32 launch");
   return R2M_OK;
 }

@@ -21,28 +21,13 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "lt_api.cuh"
 
 namespace r2m {
 
 // ------------------------------------------------------------- cuBLASLt
 
-struct LtApi {
-  void *so = nullptr;
-  decltype(&cublasLtCreate) create;
-  decltype(&cublasLtDestroy) destroy;
-  decltype(&cublasLtMatmulDescCreate) desc_create;
-  decltype(&cublasLtMatmulDescDestroy) desc_destroy;
-  decltype(&cublasLtMatmulDescSetAttribute) desc_set;
-  decltype(&cublasLtMatrixLayoutCreate) layout_create;
-  decltype(&cublasLtMatrixLayoutDestroy) layout_destroy;
-  decltype(&cublasLtMatmulPreferenceCreate) pref_create;
-  decltype(&cublasLtMatmulPreferenceDestroy) pref_destroy;
-  decltype(&cublasLtMatmulPreferenceSetAttribute) pref_set;
-  decltype(&cublasLtMatmulAlgoGetHeuristic) heuristic;
-  decltype(&cublasLtMatmul) matmul;
-};
-
-static int lt_api(LtApi **out) {
+int lt_api(LtApi **out) {
   static std::mutex mu;
   static LtApi api;
   static bool ok = false;

@@ -54,6 +54,8 @@ SIGNATURES = [
                                  ctypes.POINTER(I)]),
     ("r2m_batch_gemm_topk", I, [P, P, P, I, P, P, P]),
     ("r2m_batch_gemm_topk_noalloc", I, [P, P, I, I64, P, P, I, I, I, P, P, P]),
+    ("r2m_rescore_fp32", I, [P, I, P, I, P, P, P, I64, I, I, I, I, I, P, P, P, I, P]),
+    ("r2m_check_fp64", I, [P, I, P, P, P, I64, I, I, I, I, P, I, P, P, P, P]),
     ("r2m_plain_engine_create", I, [P, I, I64, I, I, I, I, ctypes.POINTER(P)]),
     ("r2m_plain_engine_destroy", I, [P]),
     ("r2m_plain_batch_gemm_topk", I, [P, P, I, P, P, P]),
