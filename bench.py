@@ -294,6 +294,78 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31):
     return out
 
 
+# ---------------------------------------------------------------- precision leg
+
+
+def precision_leg(dev, n_reads: int, n_sample: int, seed: int = 51):
+    """Precision form on the 100 Mbp configuration: 10 records x 10 Mbp,
+    GC 41%, 1% N runs of 100..10,000 bp, k = 150, kstep = 15 (fwd + rc,
+    ~13.3M columns, per-column scaled e4m3); reads of 150 bp with 5% iid
+    substitutions; fp8 top-64 -> FP32 rescoring -> top-20; FP64 check on
+    `n_sample` sampled rows (score error, top-20 recall)."""
+    import torch
+    import rotormap as rm
+    from rotormap import synth
+    re = rm.RopeEncoder(k=K_BASES, s=S, m=M, c=C)
+    lengths = np.full(10, 10_000_000, np.int64)
+    words, woff, nbases, runs = synth.random_genome_packed(lengths, seed=seed, gc=0.41, n_frac=0.01,
+                                                           run_min=100, run_max=10_000, device=dev)
+    heads = [f">rec{i + 1} synthetic 10 Mbp" for i in range(10)]
+    t0 = time.perf_counter()
+    idx = rm.build_index_packed(re, words, heads, woff, nbases, KSTEP, scaled=True)
+    t_index = time.perf_counter() - t0
+    meta = rm.DeviceMeta(idx, genome=words)
+    recs, offs = synth.sample_positions(nbases, runs, n_reads, K_BASES, seed + 1)
+    rw = synth.extract_reads_packed(words, woff, recs, offs, K_BASES, ERR, seed + 1)
+    dw = torch.from_numpy(rw.view(np.int32)).to(dev)
+    eng = rm.TopKEngine(idx.embeds8, k=64, rows_cap=n_reads, score="scaled", scaleB=idx.scales)
+    rm.map_precise(eng, re, meta, dw[:256])  # warm-up
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    st = torch.cuda.current_stream()
+    e0.record(st)
+    nb = n_reads
+    a8, sa = eng.a8[:nb], eng.scaleA[:nb]
+    norms = torch.empty((nb, M), dtype=torch.float32, device=dev)
+    rm.encode_frag_real_batch(a8, norms, re, dw.reshape(-1), 0, sa)
+    v8, l8 = eng.search(a8, nb, sa)
+    e1.record(st)
+    v32, l32 = rm.rescore_fp32(re, meta, dw, l8, TOPK)
+    e2.record(st)
+    torch.cuda.synchronize()
+    t_fp8, t_resc = e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
+    # FP64 check on sampled rows
+    rng = np.random.default_rng(seed + 2)
+    samp = np.sort(rng.choice(n_reads, size=n_sample, replace=False))
+    ds = torch.from_numpy(samp).to(dev)
+    cand = torch.cat([l8[ds][:, :TOPK], l32[ds]], dim=1).contiguous()
+    t0 = time.perf_counter()
+    v64, l64, c64 = rm.check_fp64(re, meta, dw[ds].contiguous(), cand)
+    t_check = time.perf_counter() - t0
+    l8s, l32s, l64 = l8[ds][:, :TOPK].cpu().numpy(), l32[ds].cpu().numpy(), l64.cpu().numpy()
+    v8s, v32s, c64 = v8[ds][:, :TOPK].cpu().numpy(), v32[ds].cpu().numpy(), c64.cpu().numpy()
+    rec = lambda a, b: float(np.mean([len(set(x) & set(y)) / TOPK for x, y in zip(a, b)]))
+    err8 = np.abs(v8s - c64[:, :TOPK])
+    err32 = np.abs(v32s - c64[:, TOPK:])
+    l32a = l32.cpu().numpy()
+    c = l32a.astype(np.int64) - 1
+    ok = (idx.col_rec[c] == recs[:, None]) & (np.abs(idx.starts[c] - (offs[:, None] + 1)) < K_BASES)
+    out = {"workload": f"100 Mbp genome (10 x 10 Mbp, GC 41%, 1% N runs), k=150 kstep=15 -> N={idx.N} columns "
+                       f"(scaled e4m3), {n_reads} reads x 150 bp (5% subs), fp8 top-64 -> FP32 rescore -> top-20",
+           "index_cols": idx.N, "reads": n_reads, "index_build_s": t_index,
+           "fp8_search_s": t_fp8, "rescore_s": t_resc,
+           "reads_per_s": n_reads / (t_fp8 + t_resc),
+           "fp64_check": {"sampled_rows": n_sample, "seconds": t_check,
+                          "top20_recall_fp8": rec(l8s, l64), "top20_recall_fp32_rescored": rec(l32s, l64),
+                          "score_abs_err_fp8": {"max": float(err8.max()), "mean": float(err8.mean())},
+                          "score_abs_err_fp32": {"max": float(err32.max()), "mean": float(err32.mean())}},
+           "mapped_frac_top20": float(ok.any(axis=1).mean())}
+    eng.close()
+    del idx, meta, words, eng
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- GPU leg
 
 
@@ -309,6 +381,9 @@ def main():
     ap.add_argument("--splits", type=int, default=0, help="force the column split count (0 = auto)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-vs-plain leg")
     ap.add_argument("--requests", type=int, default=16, help="requests in the serving leg")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision leg")
+    ap.add_argument("--precision-reads", type=int, default=100_000)
+    ap.add_argument("--precision-sample", type=int, default=1000)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -443,6 +518,8 @@ def main():
     if rank == 0:
         if world == 1 and not args.no_serving:
             line["serving"] = serving_leg(dev, args.requests)
+        if world == 1 and not args.no_precision:
+            line["precision"] = precision_leg(dev, args.precision_reads, args.precision_sample)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
