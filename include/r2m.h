@@ -132,6 +132,12 @@ int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int rdim,
                       int64_t N, int k, int rows_cap, int score_mode,
                       const r2m_tuning *tune, r2m_engine **out);
 int r2m_engine_destroy(r2m_engine *eng);
+/* Change an engine's schedule (column splits, persistent CTAs) -- the knob
+ * the autotuner of the batching form turns; grows the split workspace when
+ * the new schedule needs more (synchronizes the device in that case, so call
+ * it outside stream capture).  No reference counterpart (the reference's
+ * schedule knobs are the constructor's w / segs). */
+int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune);
 /* Bytes of device workspace the engine holds. */
 int64_t r2m_engine_workspace_bytes(const r2m_engine *eng);
 /* Device time of the last r2m_batch_gemm_topk's GEMM+top-k kernel and of

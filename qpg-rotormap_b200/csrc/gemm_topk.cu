@@ -630,6 +630,37 @@ extern "C" int r2m_engine_destroy(r2m_engine *eng) {
   return R2M_OK;
 }
 
+extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
+  R2M_REQUIRE(eng != nullptr && tune != nullptr, "null pointer");
+  const int ctas = tune->ctas > 0 ? tune->ctas : sm_count();
+  const int forced = tune->splits > 0 ? tune->splits : 0;
+  int mt_cap = (eng->rows_cap + BM - 1) / BM;
+  size_t lists = 0;
+  for (int mt = 1; mt <= mt_cap; ++mt) {
+    size_t l = (size_t)choose_splits(mt, eng->n_tiles, ctas, forced) * mt * BM;
+    if (l > lists) lists = l;
+  }
+  if (lists > eng->part_lists) {  // grow the split workspace
+    float *pv = nullptr;
+    int *pc = nullptr;
+    cudaError_t ce = cudaMalloc(&pv, lists * eng->KT * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMalloc(&pc, lists * eng->KT * sizeof(int));
+    if (ce != cudaSuccess) {
+      cudaFree(pv);
+      return fail(R2M_ENOMEM, "engine workspace allocation failed");
+    }
+    R2M_CUDA(cudaDeviceSynchronize());
+    cudaFree(eng->part_vals);
+    cudaFree(eng->part_cols);
+    eng->part_vals = pv;
+    eng->part_cols = pc;
+    eng->part_lists = lists;
+  }
+  eng->ctas = ctas;
+  eng->forced_splits = forced;
+  return R2M_OK;
+}
+
 extern "C" int64_t r2m_engine_workspace_bytes(const r2m_engine *eng) {
   if (!eng) return 0;
   return (int64_t)(eng->part_lists * eng->KT * (sizeof(float) + sizeof(int)));

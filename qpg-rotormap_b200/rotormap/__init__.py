@@ -13,6 +13,7 @@ from .fasta import FastaFragments, fasta_reads
 from .index import (FP8_FORMAT, SCALED_FORMAT, Index, RefPack, build_index, build_index_packed,
                     index_database,
                     load_index, pack_records, pack_reference, save_index, window_positions)
+from .batching import Autotuner, RaggedBatcher, bucket_rows
 from .precision import DeviceMeta, check_fp64, map_precise, rescore_fp32
 from .mapping import julia_repr_f32, map_and_count, parse_read_head, run_map, score_provenance
 

@@ -49,6 +49,7 @@ SIGNATURES = [
     ("r2m_f16_to_e4m3", I, [P, P, I64, P]),
     ("r2m_engine_create", I, [P, P, I, I64, I, I, I, ctypes.POINTER(Tuning), ctypes.POINTER(P)]),
     ("r2m_engine_destroy", I, [P]),
+    ("r2m_engine_set_tuning", I, [P, ctypes.POINTER(Tuning)]),
     ("r2m_engine_workspace_bytes", I64, [P]),
     ("r2m_engine_kernel_ms", I, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
                                  ctypes.POINTER(I)]),

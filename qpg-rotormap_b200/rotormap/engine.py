@@ -73,6 +73,12 @@ class TopKEngine:
                                       ctypes.byref(tune), ctypes.byref(h)))
         self._h = h
 
+    def set_tuning(self, splits: int = 0, ctas: int = 0, timing: bool | None = None) -> None:
+        """Change the schedule (0 = automatic).  Not during stream capture."""
+        t = Tuning(splits, ctas)
+        check(lib().r2m_engine_set_tuning(self._h, ctypes.byref(t)))
+        self.splits, self.ctas = splits, ctas
+
     def kernel_ms(self):
         """(gemm_ms, merge_ms, splits) of the last search (timing engines only)."""
         g, m, sp = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
