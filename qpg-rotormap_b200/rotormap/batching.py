@@ -35,8 +35,12 @@ def bucket_rows(n: int) -> int:
 class Autotuner:
     """Picks (splits, ctas) for an engine and row count by timing candidates."""
 
-    def __init__(self, cache_path: str | None = None, reps: int = 2):
+    def __init__(self, cache_path: str | None = None, reps: int = 2, proxy_cols: int = 0):
         self.reps = reps
+        # >0: time candidates on an engine over the first proxy_cols index
+        # columns (the schedule's wave behaviour depends on read tiles x splits
+        # vs CTAs, not on the column count), then apply the winner
+        self.proxy_cols = proxy_cols
         self.cache: dict = {}
         self.path = Path(cache_path) if cache_path else None
         if self.path and self.path.exists():
@@ -68,20 +72,27 @@ class Autotuner:
             return s, c
         sms = torch.cuda.get_device_properties(eng.B.device).multi_processor_count
         st = stream or torch.cuda.current_stream(eng.B.device)
+        target = eng
+        if 0 < self.proxy_cols < eng.N:
+            from .engine import TopKEngine
+            sb = eng.scaleB[:self.proxy_cols] if eng.scaleB is not None else None
+            target = TopKEngine(eng.B[:self.proxy_cols], k=eng.k, rows_cap=eng.rows_cap, score=eng.score, scaleB=sb)
         best, best_ms = (0, 0), float("inf")
         for s, c in self.candidates(rows, eng.N, sms):
-            eng.set_tuning(s, c)
-            eng.search(A8, rows, scaleA, stream=st)  # warm
+            target.set_tuning(s, c)
+            target.search(A8, rows, scaleA, stream=st)  # warm
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
             for _ in range(self.reps):
-                eng.search(A8, rows, scaleA, stream=st)
+                target.search(A8, rows, scaleA, stream=st)
             e1.record(st)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / self.reps
             self.log.append({"rows": rows, "splits": s, "ctas": c, "ms": ms})
             if ms < best_ms:
                 best, best_ms = (s, c), ms
+        if target is not eng:
+            target.close()
         eng.set_tuning(*best)
         self.cache[k] = list(best)
         if self.path:
