@@ -536,9 +536,8 @@ def main():
     e2e_s = sum(e2e_t) / len(e2e_t)
 
     if world > 1:
-        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(t[0]), float(t[1])
+        from rotormap.dist import max_over_ranks
+        ms, e2e_s = max_over_ranks([ms, e2e_s], device=dev)
 
     if rank == 0:
         pk, basis = peaks()
