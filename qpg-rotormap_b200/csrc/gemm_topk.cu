@@ -357,6 +357,274 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
+// ------------------------------------------------------------------
+// 2-SM variant: a CTA pair (cluster of 2) computes a 256-read x 256-column
+// tile with tcgen05.mma.cta_group::2 (M = 256, N = 256, K = 32).  Each CTA
+// loads its own 128 read rows and its own 128 of the 256 index columns per
+// stage (32 KiB instead of 48 KiB per CTA), so a CTA pulls 2/3 of the
+// single-CTA kernel's operand bytes per FLOP.  The leader CTA (rank 0)
+// issues the MMAs; both CTAs' TMA loads complete on the leader's stage
+// barrier; the leader's commits release both CTAs' stages and signal both
+// CTAs' accumulators; each CTA's epilogue drains its own 128 TMEM lanes (all
+// 256 columns) and arrives on the leader's accumulator-empty barrier.  No
+// multicast is used anywhere.
+constexpr int STAGES2 = 6;
+constexpr int HALF_TILE = 128 * BK;  // 16 KiB
+
+template <int KT>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_gemm_topk2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem =
+      reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + STAGES2 * HALF_TILE;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sB + STAGES2 * HALF_TILE);
+  uint64_t *empty = full + STAGES2;
+  uint64_t *acc_full = empty + STAGES2;
+  uint64_t *acc_empty = acc_full + 2;
+  uint64_t *drain = acc_empty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // 128 x 33 floats
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES2; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 8);  // 4 epilogue warps x 2 CTAs (leader's copy is used)
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_slot, TMEM_COLS);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs' barriers are initialised before any remote arrive
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const int num_units = g.num_m_tiles * g.splits;
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer (both CTAs)
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      long long issued = 0;
+      bool ok = true;
+      for (int u = pair; ok && u < num_units; u += npairs) {
+        const int mt = u % g.num_m_tiles, sp = u / g.num_m_tiles;
+        const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
+        for (int t = t0; ok && t < t1; ++t) {
+          for (int kb = 0; kb < g.num_kb; ++kb) {
+            if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, abort_flag, WAIT_LIMIT)) {
+              if (!*abort_flag) atomicExch(g.err, kErrTimeoutEmpty);
+              *abort_flag = 1;
+              ok = false;
+              break;
+            }
+            const uint32_t fbar = mapa_shared(smem_u32(&full[stage]), 0);
+            if (leader) mbar_arrive_expect_tx(&full[stage], 4 * HALF_TILE);
+            tma_load_2d_pair(sA + stage * HALF_TILE, &tmA, fbar, kb * BK, mt * 256 + (int)rank * 128);
+            tma_load_2d_pair(sB + stage * HALF_TILE, &tmB, fbar, kb * BK, t * BN + (int)rank * 128);
+            ++issued;
+            if (++stage == STAGES2) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+        }
+      }
+      if (!ok && leader) {
+        int nlast = issued < STAGES2 ? (int)issued : STAGES2;
+        for (int j = 1; j <= nlast; ++j) {
+          int s = stage - j;
+          uint32_t ph = phase;
+          if (s < 0) {
+            s += STAGES2;
+            ph ^= 1u;
+          }
+          long long c0 = clock64();
+          while (!mbar_try_wait(&full[s], ph) && clock64() - c0 < WAIT_LIMIT) {
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer (leader CTA)
+    if (lane == 0 && leader) {
+      const uint32_t idesc = idesc_e4m3_f32(256, BN);
+      int stage = 0;
+      uint32_t phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true;
+      for (int u = pair; ok && u < num_units; u += npairs) {
+        const int sp = u / g.num_m_tiles;
+        const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
+        for (int t = t0; ok && t < t1; ++t) {
+          if (!mbar_wait_bounded(&acc_empty[acc], acc_phase ^ 1u, abort_flag, WAIT_LIMIT)) {
+            if (!*abort_flag) atomicExch(g.err, kErrTimeoutAccEmpty);
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+          for (int kb = 0; kb < g.num_kb; ++kb) {
+            if (!mbar_wait_bounded(&full[stage], phase, abort_flag, WAIT_LIMIT)) {
+              if (!*abort_flag) atomicExch(g.err, kErrTimeoutFull);
+              *abort_flag = 1;
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA + stage * HALF_TILE);
+            const uint32_t b0 = smem_u32(sB + stage * HALF_TILE);
+#pragma unroll
+            for (int kk = 0; kk < BK / 32; ++kk)
+              mma_f8_pair(d_tmem, smem_desc_sw128(a0 + kk * 32), smem_desc_sw128(b0 + kk * 32), idesc,
+                          (kb | kk) != 0 ? 1u : 0u);
+            const uint32_t eb = smem_u32(&empty[stage]);
+            mma_commit_pair(mapa_shared(eb, 0));
+            mma_commit_pair(mapa_shared(eb, 1));
+            if (++stage == STAGES2) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+          if (!ok) break;
+          const uint32_t fb = smem_u32(&acc_full[acc]);
+          mma_commit_pair(mapa_shared(fb, 0));
+          mma_commit_pair(mapa_shared(fb, 1));
+          acc ^= 1;
+          if (acc == 0) acc_phase ^= 1u;
+        }
+      }
+      mma_commit_pair(mapa_shared(smem_u32(drain), 0));
+      long long c0 = clock64();
+      while (!mbar_try_wait(drain, 0) && clock64() - c0 < WAIT_LIMIT) {
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------ epilogue (both CTAs)
+    const int quarter = warp & 3;
+    const int row_in_tile = quarter * 32 + lane;
+    float *scratch = scratch_all + (threadIdx.x - 64) * 33;
+    const bool f16 = g.score_mode == R2M_SCORE_F16;
+    const bool scaled = g.score_mode == R2M_SCORE_SCALED;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    Reservoir<KT> R;
+    for (int u = pair; ok && u < num_units; u += npairs) {
+      const int mt = u % g.num_m_tiles, sp = u / g.num_m_tiles;
+      const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
+      R.reset();
+      for (int t = t0; t < t1; ++t) {
+        bool w = mbar_wait_bounded(&acc_full[acc], acc_phase, abort_flag, WAIT_LIMIT);
+        if (__any_sync(FULL, !w)) {
+          if (lane == 0 && !*abort_flag) atomicExch(g.err, kErrTimeoutAccFull);
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
+        const long long colbase = (long long)t * BN;
+        const bool tail = colbase + BN > g.N;
+#pragma unroll 1
+        for (int ch = 0; ch < BN / 32; ++ch) {
+          float v[32];
+          __syncwarp();
+          tmem_ld32(taddr + ch * 32, v);
+          tmem_wait_ld();
+          const long long c0 = colbase + ch * 32;
+          if (scaled) {
+            if (!tail) {
+              const float4 *sb = reinterpret_cast<const float4 *>(g.scaleB + c0);
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                float4 s4 = __ldg(sb + q);
+                v[4 * q] *= s4.x;
+                v[4 * q + 1] *= s4.y;
+                v[4 * q + 2] *= s4.z;
+                v[4 * q + 3] *= s4.w;
+              }
+            } else {
+#pragma unroll
+              for (int j = 0; j < 32; ++j) v[j] = (c0 + j < g.N) ? v[j] * __ldg(g.scaleB + c0 + j) : v[j];
+            }
+          }
+          if (tail) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j >= g.N) v[j] = -INFINITY;
+          }
+          float mx = v[0];
+#pragma unroll
+          for (int j = 1; j < 32; ++j) mx = fmaxf(mx, v[j]);
+          if (f16) mx = round_f16(mx);
+          if (mx > R.thr) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) scratch[j] = v[j];
+#pragma unroll 1
+            for (int j = 0; j < 32; ++j) {
+              float x = scratch[j];
+              if (f16) x = round_f16(x);
+              if (x > R.thr) R.insert(x, (int)(c0 + j));
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[acc]), 0));
+        acc ^= 1;
+        if (acc == 0) acc_phase ^= 1u;
+      }
+      if (!ok) break;
+      const int row = mt * 256 + (int)rank * 128 + row_in_tile;
+      if (row < g.nb) {
+        float *pv = g.part_vals + ((size_t)sp * g.mpad + row) * KT;
+        int *pc = g.part_cols + ((size_t)sp * g.mpad + row) * KT;
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          pv[j] = R.v[j];
+          pc[j] = R.c[j];
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // the leader's MMAs touch the peer's smem and TMEM until here
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, TMEM_COLS);
+  }
+}
+
 // Merge the per-split sorted lists of every row into its final top-k:
 // one warp per row, k rounds of a warp arg-max over the list heads.
 __global__ void k_merge_splits(const float *__restrict__ pv, const int *__restrict__ pc, int splits,
@@ -523,6 +791,54 @@ static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmA
   return R2M_OK;
 }
 
+static size_t gemm2_smem_bytes() {
+  return 1024 + (size_t)STAGES2 * 2 * HALF_TILE + (2 * STAGES2 + 5) * 8 + 16 + (size_t)BM * 33 * sizeof(float);
+}
+
+template <int KT>
+static int launch_gemm2(const CUtensorMap &mA, const CUtensorMap &mB, const GemmArgs &g, int pairs,
+                        cudaStream_t st) {
+  size_t smem = gemm2_smem_bytes();
+  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk2<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * pairs, 1, 1);
+  cfg.blockDim = dim3(THREADS, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  R2M_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_topk2<KT>, mA, mB, g));
+  return R2M_OK;
+}
+
+// Which kernel a batch of nb reads runs on: 1 = one CTA per 128-read tile,
+// 2 = CTA pairs per 256-read tile.  mode 0 (auto) uses pairs above 128 reads.
+static int kernel_kind(int mode, int nb) {
+  if (mode == 1) return 1;
+  if (mode == 2) return 2;
+  return nb > BM ? 2 : 1;
+}
+
+// Split lists the workspace must hold for any batch height up to rows_cap.
+static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int mode) {
+  size_t lists = 0;
+  for (int nb = BM; nb < rows_cap + BM; nb += BM) {
+    int h = nb < rows_cap ? nb : rows_cap;
+    int kind = kernel_kind(mode, h);
+    int tile = kind == 2 ? 256 : BM;
+    int mt = (h + tile - 1) / tile;
+    int c = kind == 2 ? (ctas / 2 > 0 ? ctas / 2 : 1) : ctas;
+    size_t l = (size_t)choose_splits(mt, n_tiles, c, forced) * mt * tile;
+    if (l > lists) lists = l;
+  }
+  return lists;
+}
+
 }  // namespace r2m
 
 using namespace r2m;
@@ -539,6 +855,8 @@ struct r2m_engine {
   int forced_splits;
   int n_tiles;
   CUtensorMap mapB;
+  CUtensorMap mapB128;  // 128-row box for the CTA-pair kernel
+  int mode;             // 0 auto, 1 single-CTA kernel, 2 CTA-pair kernel
   float *part_vals;
   int *part_cols;
   size_t part_lists;  // capacity in lists (rows x splits)
@@ -577,6 +895,8 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   e->ctas = (tune && tune->ctas > 0) ? tune->ctas : sm_count();
   e->forced_splits = (tune && tune->splits > 0) ? tune->splits : 0;
   e->timing = tune && tune->reserved[0] != 0;
+  e->mode = tune ? tune->reserved[1] : 0;
+  if (e->mode < 0 || e->mode > 2) e->mode = 0;
   e->last_splits = 0;
   if (e->timing) {
     for (int i = 0; i < 3; ++i) {
@@ -589,18 +909,13 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   }
   e->n_tiles = (int)((N + BN - 1) / BN);
   rc = make_map(&e->mapB, d_B, N, rdim, BN);
+  if (!rc) rc = make_map(&e->mapB128, d_B, N, rdim, 128);
   if (rc) {
     delete e;
     return rc;
   }
   // workspace: the largest (read tiles x splits) any batch height can ask for
-  int mt_cap = (rows_cap + BM - 1) / BM;
-  size_t lists = 0;
-  for (int mt = 1; mt <= mt_cap; ++mt) {
-    int s = choose_splits(mt, e->n_tiles, e->ctas, e->forced_splits);
-    size_t l = (size_t)s * mt * BM;
-    if (l > lists) lists = l;
-  }
+  size_t lists = lists_needed(rows_cap, e->n_tiles, e->ctas, e->forced_splits, e->mode);
   e->part_lists = lists;
   cudaError_t ce = cudaMalloc(&e->part_vals, lists * e->KT * sizeof(float));
   if (ce == cudaSuccess) ce = cudaMalloc(&e->part_cols, lists * e->KT * sizeof(int));
@@ -634,12 +949,8 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   R2M_REQUIRE(eng != nullptr && tune != nullptr, "null pointer");
   const int ctas = tune->ctas > 0 ? tune->ctas : sm_count();
   const int forced = tune->splits > 0 ? tune->splits : 0;
-  int mt_cap = (eng->rows_cap + BM - 1) / BM;
-  size_t lists = 0;
-  for (int mt = 1; mt <= mt_cap; ++mt) {
-    size_t l = (size_t)choose_splits(mt, eng->n_tiles, ctas, forced) * mt * BM;
-    if (l > lists) lists = l;
-  }
+  const int mode = (tune->reserved[1] >= 0 && tune->reserved[1] <= 2) ? tune->reserved[1] : 0;
+  size_t lists = lists_needed(eng->rows_cap, eng->n_tiles, ctas, forced, mode);
   if (lists > eng->part_lists) {  // grow the split workspace
     float *pv = nullptr;
     int *pc = nullptr;
@@ -658,6 +969,7 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   }
   eng->ctas = ctas;
   eng->forced_splits = forced;
+  eng->mode = mode;
   return R2M_OK;
 }
 
@@ -678,30 +990,43 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   CUtensorMap mapA;
   int rc = make_map(&mapA, d_A, nb, eng->rdim, BM);
   if (rc) return rc;
+  const int kind = kernel_kind(eng->mode, nb);
+  const int tile = kind == 2 ? 256 : BM;
+  const int ctas_eff = kind == 2 ? (eng->ctas / 2 > 0 ? eng->ctas / 2 : 1) : eng->ctas;
   GemmArgs g;
   g.nb = nb;
-  g.num_m_tiles = (nb + BM - 1) / BM;
+  g.num_m_tiles = (nb + tile - 1) / tile;
   g.N = eng->N;
   g.n_tiles = eng->n_tiles;
-  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, eng->ctas, eng->forced_splits);
+  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits);
   g.num_kb = (eng->rdim + BK - 1) / BK;
   g.score_mode = eng->score_mode;
-  g.mpad = g.num_m_tiles * BM;
+  g.mpad = g.num_m_tiles * tile;
   g.scaleB = eng->scaleB;
   g.part_vals = eng->part_vals;
   g.part_cols = eng->part_cols;
   g.err = eng->err;
   if ((size_t)g.splits * g.mpad > eng->part_lists) return fail(R2M_ESTATE, "engine workspace too small");
   long long units = (long long)g.num_m_tiles * g.splits;
-  int ctas = (int)(units < eng->ctas ? units : eng->ctas);
+  int ctas = (int)(units < ctas_eff ? units : ctas_eff);
   eng->last_splits = g.splits;
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[0], st));
-  switch (eng->KT) {
-    case 8: rc = launch_gemm<8>(mapA, eng->mapB, g, ctas, st); break;
-    case 16: rc = launch_gemm<16>(mapA, eng->mapB, g, ctas, st); break;
-    case 20: rc = launch_gemm<20>(mapA, eng->mapB, g, ctas, st); break;
-    case 32: rc = launch_gemm<32>(mapA, eng->mapB, g, ctas, st); break;
-    default: rc = launch_gemm<64>(mapA, eng->mapB, g, ctas, st); break;
+  if (kind == 2) {
+    switch (eng->KT) {
+      case 8: rc = launch_gemm2<8>(mapA, eng->mapB128, g, ctas, st); break;
+      case 16: rc = launch_gemm2<16>(mapA, eng->mapB128, g, ctas, st); break;
+      case 20: rc = launch_gemm2<20>(mapA, eng->mapB128, g, ctas, st); break;
+      case 32: rc = launch_gemm2<32>(mapA, eng->mapB128, g, ctas, st); break;
+      default: rc = launch_gemm2<64>(mapA, eng->mapB128, g, ctas, st); break;
+    }
+  } else {
+    switch (eng->KT) {
+      case 8: rc = launch_gemm<8>(mapA, eng->mapB, g, ctas, st); break;
+      case 16: rc = launch_gemm<16>(mapA, eng->mapB, g, ctas, st); break;
+      case 20: rc = launch_gemm<20>(mapA, eng->mapB, g, ctas, st); break;
+      case 32: rc = launch_gemm<32>(mapA, eng->mapB, g, ctas, st); break;
+      default: rc = launch_gemm<64>(mapA, eng->mapB, g, ctas, st); break;
+    }
   }
   if (rc) return rc;
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[1], st));

@@ -31,12 +31,13 @@ def unit_e4m3(rng, n, rdim):
     return orc.quantize_parity(x)
 
 
-def run_engine(A8, B8, k, score="f16", scaleA=None, scaleB=None, splits=0, ctas=0):
+def run_engine(A8, B8, k, score="f16", scaleA=None, scaleB=None, splits=0, ctas=0, kernel="auto"):
     B = torch.from_numpy(B8).cuda()
     A = torch.from_numpy(A8).cuda()
     sb = torch.from_numpy(scaleB).cuda() if scaleB is not None else None
     sa = torch.from_numpy(scaleA).cuda() if scaleA is not None else None
-    eng = rm.TopKEngine(B, k=k, rows_cap=A8.shape[0], score=score, scaleB=sb, splits=splits, ctas=ctas)
+    eng = rm.TopKEngine(B, k=k, rows_cap=A8.shape[0], score=score, scaleB=sb, splits=splits, ctas=ctas,
+                        kernel=kernel)
     v, l = eng.search(A, A8.shape[0], sa)
     torch.cuda.synchronize()
     from rotormap._lib import check, lib
@@ -52,13 +53,14 @@ SHAPES = [(64, 100), (257, 128), (1000, 333), (1, 4096), (511, 2048), (2048, 163
 
 @pytest.mark.parametrize("nb,N", SHAPES)
 @pytest.mark.parametrize("score", ["f16", "f32"])
-def test_topk_exact_integer_scores(nb, N, score):
+@pytest.mark.parametrize("kernel", ["1sm", "2sm"])
+def test_topk_exact_integer_scores(nb, N, score, kernel):
     rng = np.random.default_rng(nb * 7 + N)
     rdim = 256
     A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
     B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
     k = 20
-    v, l = run_engine(A8, B8, k, score)
+    v, l = run_engine(A8, B8, k, score, kernel=kernel)
     ov, ol = orc.topk_e4m3(A8, B8, k, 0 if score == "f16" else 1)
     assert np.array_equal(v, ov)
     assert np.array_equal(l, ol)  # ties broken by ascending column, exactly
@@ -74,24 +76,26 @@ def test_topk_k_values(k):
     assert np.array_equal(v, ov) and np.array_equal(l, ol)
 
 
-@pytest.mark.parametrize("splits,ctas", [(1, 1), (3, 2), (7, 5), (0, 3), (128, 0)])
-def test_topk_schedules(splits, ctas):
-    """Forced column splits / few CTAs: several work units per CTA reuse the
-    TMEM double buffer across units."""
+@pytest.mark.parametrize("splits,ctas", [(1, 2), (3, 2), (7, 6), (0, 4), (128, 0)])
+@pytest.mark.parametrize("kernel", ["1sm", "2sm"])
+def test_topk_schedules(splits, ctas, kernel):
+    """Forced column splits / few CTAs: several work units per CTA (pair)
+    reuse the TMEM double buffer across units."""
     rng = np.random.default_rng(splits + 10 * ctas)
     A8, _ = int_e4m3(rng, (300, 256))
     B8, _ = int_e4m3(rng, (9000, 256))
-    v, l = run_engine(A8, B8, 20, splits=splits, ctas=ctas)
+    v, l = run_engine(A8, B8, 20, splits=splits, ctas=ctas, kernel=kernel)
     ov, ol = orc.topk_e4m3(A8, B8, 20, 0)
     assert np.array_equal(v, ov) and np.array_equal(l, ol)
 
 
 @pytest.mark.parametrize("rdim", [16, 48, 128, 384, 2048])
-def test_topk_rdim_tails(rdim):
+@pytest.mark.parametrize("kernel", ["1sm", "2sm"])
+def test_topk_rdim_tails(rdim, kernel):
     rng = np.random.default_rng(rdim)
-    A8, _ = int_e4m3(rng, (100, rdim), -1, 1)
+    A8, _ = int_e4m3(rng, (300, rdim), -1, 1)
     B8, _ = int_e4m3(rng, (3000, rdim), -1, 1)
-    v, l = run_engine(A8, B8, 20, "f32")
+    v, l = run_engine(A8, B8, 20, "f32", kernel=kernel)
     ov, ol = orc.topk_e4m3(A8, B8, 20, 1)
     assert np.array_equal(v, ov) and np.array_equal(l, ol)
 
