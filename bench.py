@@ -559,7 +559,10 @@ def main():
                        "l2": "inputs > L2 (34 GB index streamed every step)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_gemm_topk (fused tcgen05 fp8 GEMM + top-20)",
+                         "traffic_note": "DRAM is ~1.5% busy (tensor/power-bound kernel); per-launch DRAM bytes "
+                                         "of a small case are in profiles/k_gemm_topk2_16384x1048576_full.md",
+                         "kernel": ("k_gemm_topk2 (CTA-pair tcgen05 fp8 GEMM + fused top-20)" if nq > 128 else
+                                    "k_gemm_topk (single-CTA tcgen05 fp8 GEMM + fused top-20)"),
                          "peak_basis": f"dense fp8 = 2 x {basis} sustained bf16 "
                                        f"({pk['bf16_tflops_sustained']} TFLOP/s)"},
             "encoder": {"ms": sum(enc_ms) / len(enc_ms),
