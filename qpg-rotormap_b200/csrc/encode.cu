@@ -156,6 +156,22 @@ __device__ __forceinline__ void store16(void *row, int i0, const float (&v)[16])
   }
 }
 
+// 16 values -> e4m3(fp16(x)) (the reference's fp16 stream quantised by
+// f32_to_f8 of the widened value) with one cvt per pair, 16-byte store.
+__device__ __forceinline__ void store16_f16e4m3(void *row, int i0, const float (&v)[16]) {
+  uint32_t w[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    __half2 h01 = __floats2half2_rn(v[4 * q], v[4 * q + 1]);
+    __half2 h23 = __floats2half2_rn(v[4 * q + 2], v[4 * q + 3]);
+    uint16_t lo, hi;
+    asm("cvt.rn.satfinite.e4m3x2.f16x2 %0, %1;" : "=h"(lo) : "r"(*reinterpret_cast<uint32_t *>(&h01)));
+    asm("cvt.rn.satfinite.e4m3x2.f16x2 %0, %1;" : "=h"(hi) : "r"(*reinterpret_cast<uint32_t *>(&h23)));
+    w[q] = (uint32_t)lo | ((uint32_t)hi << 16);
+  }
+  *reinterpret_cast<uint4 *>(reinterpret_cast<uint8_t *>(row) + i0) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 template <int OUT>
 __device__ __forceinline__ void store1(void *row, int i, float v) {
   if constexpr (OUT == R2M_OUT_F32) {
@@ -187,7 +203,7 @@ __device__ __forceinline__ float out_value(const EncParams &P, const float *hist
 // G-homopolymer bins zeroed, modes 2/3 reshaped; `nrmv` receives the divisor
 // of every copy (index 0 for mode 0) and `norms_out` the reference's norms
 // row.  The normalised value of split element i is hist[...]/nrmv[...].
-__device__ void fragment_hist(const EncParams &P, const float2 *table, float *hist, uint16_t *cs,
+__device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *table, float *hist, uint16_t *cs,
                               const uint32_t *words, float *nrmv, float *norms_out) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
@@ -216,20 +232,32 @@ __device__ void fragment_hist(const EncParams &P, const float2 *table, float *hi
       uint32_t cbin = cs[p];
       unsigned grp = __match_any_sync(amask, cbin);
       if (lane == __ffs(grp) - 1) {
-        for (int idm = 0; idm < P.m; ++idm) {
-          float *h = hist + 2 * (cbin * P.m + idm);
-          float re = h[0], im = h[1];
-          const float2 *tb = table + (size_t)idm * P.nw + b0;
-          unsigned g = grp;
-          while (g) {
-            int j = __ffs(g) - 1;
-            g &= g - 1;
-            float2 ph = tb[j];
-            re += ph.x;
-            im += ph.y;
+        if (P.m == 4 && grp == (1u << lane)) {
+          // common case: a window alone in its bin within the batch
+          float4 *h = reinterpret_cast<float4 *>(hist + 2 * (cbin * 4));
+          float4 h01 = h[0], h23 = h[1];
+          const float2 p0 = table[b0 + lane], p1 = table[(size_t)P.nw + b0 + lane];
+          const float2 p2 = table[2 * (size_t)P.nw + b0 + lane], p3 = table[3 * (size_t)P.nw + b0 + lane];
+          h01.x += p0.x; h01.y += p0.y; h01.z += p1.x; h01.w += p1.y;
+          h23.x += p2.x; h23.y += p2.y; h23.z += p3.x; h23.w += p3.y;
+          h[0] = h01;
+          h[1] = h23;
+        } else {
+          for (int idm = 0; idm < P.m; ++idm) {
+            float *h = hist + 2 * (cbin * P.m + idm);
+            float re = h[0], im = h[1];
+            const float2 *tb = table + (size_t)idm * P.nw + b0;
+            unsigned g = grp;
+            while (g) {
+              int j = __ffs(g) - 1;
+              g &= g - 1;
+              float2 ph = tb[j];
+              re += ph.x;
+              im += ph.y;
+            }
+            h[0] = re;
+            h[1] = im;
           }
-          h[0] = re;
-          h[1] = im;
         }
       }
     }
@@ -257,18 +285,33 @@ __device__ void fragment_hist(const EncParams &P, const float2 *table, float *hi
   float part[8];
 #pragma unroll
   for (int t = 0; t < 8; ++t) part[t] = 0.f;
-  for (int b = lane; b < P.nbin; b += 32) {
-    float re = hist[2 * b], im = hist[2 * b + 1];
-    float e = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
-    int t = b % P.m;
+  if ((32 % P.m) == 0) {
+    // every bin of this lane (b = lane + 32j) belongs to copy lane % m: one
+    // accumulator, then a butterfly over the lanes of the same copy (the
+    // lanes of other copies would only add zeros, so the sums are the same)
+    float acc = 0.f;
+    const float2 *h2 = reinterpret_cast<const float2 *>(hist);
+    for (int b = lane; b < P.nbin; b += 32) {
+      float2 z = h2[b];
+      acc += __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
+    }
+    for (int o = 16; o >= P.m; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (q == t) part[q] += e;
-  }
+    for (int q = 0; q < 8; ++q) part[q] = __shfl_sync(FULL, acc, q < P.m ? q : 0);
+  } else {
+    for (int b = lane; b < P.nbin; b += 32) {
+      float re = hist[2 * b], im = hist[2 * b + 1];
+      float e = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
+      int t = b % P.m;
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < 8; ++q)
+        if (q == t) part[q] += e;
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part[q] += __shfl_xor_sync(FULL, part[q], o);
+    for (int q = 0; q < 8; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part[q] += __shfl_xor_sync(FULL, part[q], o);
+    }
   }
   if (lane == 0) {
     if (P.normalize == 0) {
@@ -301,6 +344,71 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
   fragment_hist(P, table, hist, cs, words, nrmv, norms_out);
+  if (P.normalize == 0 && (P.nbin % 16) == 0 && P.nbin >= 16) {
+    // 16 bins per lane chunk: divide in place (one division per value), then
+    // convert and store the chunk's Re and Im runs (16 values each)
+    const float nrm = nrmv[0];
+    // x / nrm for every value with one reciprocal: y = RN(1/nrm), q0 = x*y,
+    // r = x - q0*nrm (exact with FMA), q = RN(q0 + r*y) is the correctly
+    // rounded quotient (Markstein's theorem) -- the same value as x / nrm
+    const float y = __frcp_rn(nrm);
+    auto divn = [&](float x) {
+      float q0 = x * y;
+      float r = fmaf(-q0, nrm, x);
+      return fmaf(r, y, q0);
+    };
+    const int nchunk = P.nbin >> 4;
+    float amax = 0.f;
+    for (int j = lane; j < nchunk; j += 32) {
+      float4 *h4 = reinterpret_cast<float4 *>(hist + 32 * j);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        float4 t = h4[q];
+        t.x = divn(t.x);
+        t.y = divn(t.y);
+        t.z = divn(t.z);
+        t.w = divn(t.w);
+        if constexpr (OUT == R2M_OUT_E4M3_SCALED)
+          amax = fmaxf(amax, fmaxf(fmaxf(fabsf(t.x), fabsf(t.y)), fmaxf(fabsf(t.z), fabsf(t.w))));
+        h4[q] = t;
+      }
+    }
+    float scale = 1.0f;
+    if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(FULL, amax, o));
+      scale = amax > 0.f ? 448.0f / amax : 1.0f;
+      if (lane == 0) *scale_out = amax > 0.f ? amax / 448.0f : 0.0f;
+    }
+    for (int j = lane; j < nchunk; j += 32) {
+      const float4 *h4 = reinterpret_cast<const float4 *>(hist + 32 * j);
+      float re[16], im[16];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        float4 t = h4[q];
+        re[2 * q] = t.x;
+        im[2 * q] = t.y;
+        re[2 * q + 1] = t.z;
+        im[2 * q + 1] = t.w;
+      }
+      if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          re[e] *= scale;
+          im[e] *= scale;
+        }
+      }
+      if constexpr (OUT == R2M_OUT_E4M3) {
+        store16_f16e4m3(row, 16 * j, re);
+        store16_f16e4m3(row, P.nbin + 16 * j, im);
+      } else {
+        store16<OUT>(row, 16 * j, re);
+        store16<OUT>(row, P.nbin + 16 * j, im);
+      }
+    }
+    __syncwarp();
+    return;
+  }
   // output pass (amax first for the scaled form)
   float scale = 1.0f;
   if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
