@@ -247,7 +247,33 @@ int64_t r2m_reads_count(const r2m_reads *r);
 const uint32_t *r2m_reads_words(const r2m_reads *r);
 /* Header i (not NUL-terminated); its byte length in *len. */
 const char *r2m_reads_header(const r2m_reads *r, int64_t i, size_t *len);
+/* Bulk header access for hosts that convert many headers at once: every
+ * header followed by one '\n' (headers never contain '\n'), total byte
+ * length in *total_len, and the r2m_reads_count(r) + 1 byte offsets where
+ * each header starts in that blob. */
+const char *r2m_reads_header_blob(const r2m_reads *r, size_t *total_len);
+const size_t *r2m_reads_header_offsets(const r2m_reads *r);
 void r2m_reads_free(r2m_reads *r);
+
+/* ---------------------------------------------------------- device FASTA */
+
+typedef struct r2m_dreads r2m_dreads;
+
+/* Device counterpart of r2m_fasta_reads (RotorMap/fasta/reader.jl:321-350):
+ * d_data is `len` FASTA bytes in device memory.  Same kept records, in file
+ * order, with the same words; headers come back as byte spans into d_data
+ * (headers are [spans[2i], spans[2i+1]) ).  Runs on `stream` and
+ * synchronises it twice (record count, kept count).  Free with
+ * r2m_dreads_free. */
+int r2m_fasta_reads_device(const void *d_data, size_t len, int k, r2m_stream_t stream, r2m_dreads **out);
+int64_t r2m_dreads_count(const r2m_dreads *r);
+/* device, r2m_dreads_count(r) x cld(k,16) words */
+const uint32_t *r2m_dreads_words(const r2m_dreads *r);
+/* device, r2m_dreads_count(r) x 2 int64 header byte spans */
+const int64_t *r2m_dreads_spans(const r2m_dreads *r);
+/* device, every kept header followed by one '\n' (total bytes in *total_len) */
+const uint8_t *r2m_dreads_header_blob(const r2m_dreads *r, size_t *total_len);
+void r2m_dreads_free(r2m_dreads *r);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,41 @@ int sm_count() {
   return g_sm[dev];
 }
 
+// Stream-ordered scratch comes from one library pool per device that keeps
+// up to kPoolKeepBytes mapped across synchronisations (the default pool
+// returns freed memory to the OS at every sync, so a call that allocates
+// after a sync would otherwise map its scratch afresh each time).
+static constexpr uint64_t kPoolKeepBytes = 1ull << 30;
+static cudaMemPool_t g_pool[kMaxDev] = {};
+
+cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t st) {
+  *p = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaMallocAsync(p, bytes, st);
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_pool[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t np;
+      if ((e = cudaMemPoolCreate(&np, &props)) != cudaSuccess) return e;
+      uint64_t keep = kPoolKeepBytes;
+      if ((e = cudaMemPoolSetAttribute(np, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+        cudaMemPoolDestroy(np);
+        return e;
+      }
+      g_pool[dev] = np;
+    }
+    pool = g_pool[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
 int device_error_word(uint32_t **out) {
   int dev = 0;
   R2M_CUDA(cudaGetDevice(&dev));

@@ -35,6 +35,9 @@ inline cudaStream_t as_stream(r2m_stream_t s) { return (cudaStream_t)s; }
 
 // Number of SMs of the current device (cached per device).
 int sm_count();
+// Stream-ordered allocation from the library's per-device pool (freed with
+// cudaFreeAsync); the pool keeps up to 1 GiB mapped between calls.
+cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t st);
 
 // Device-side error word written by kernels whose bounded waits gave up.
 // Returns a device pointer to one uint32 per device (allocated once).

@@ -31,17 +31,20 @@ struct r2m_reads {
   int k = 0, W = 0;
   std::vector<uint32_t> words;
   std::vector<size_t> hoff;  // header offsets into `heads` (n+1 entries)
-  std::string heads;
+  std::string heads;         // every header followed by '\n'
 };
 
 namespace {
 
+// code[b]: the base's 2-bit code; '\n' and '\r' map to kSkip (not a base)
+constexpr uint8_t kSkip = 0x80;
 struct Lut {
   uint8_t code[256];
   Lut() {
     for (int i = 0; i < 256; ++i) code[i] = 2;
     code[(int)'A'] = 0; code[(int)'C'] = 1; code[(int)'G'] = 2; code[(int)'T'] = 3;
     code[(int)'a'] = 0; code[(int)'c'] = 1; code[(int)'g'] = 2; code[(int)'t'] = 3;
+    code[(int)'\n'] = kSkip; code[(int)'\r'] = kSkip;
   }
 };
 const Lut kLut;
@@ -78,21 +81,43 @@ void parse_range(const char *d, size_t n, size_t lo, size_t hi, int k, Part &out
   size_t s = lo;
   while (s < hi) {
     size_t e = next_rec(d, s + 1, n);
-    size_t h = s;
-    while (h < e && d[h] != '\n') ++h;
-    if (h == e) {  // header not closed before the next record / EOF
+    const void *nl = memchr(d + s, '\n', e - s);
+    if (!nl) {  // header not closed before the next record / EOF
       out.stop = true;
       return;
     }
+    size_t h = (size_t)((const char *)nl - d);
     size_t hend = h;  // exclusive
     if (hend > s && d[hend - 1] == '\r') --hend;
-    // collect the first k bases of [h+1, e)
+    // collect the first k bases of [h+1, e): 16 bytes per step while none
+    // of them is a line break, byte by byte otherwise
     std::fill(w.begin(), w.end(), 0u);
     int bases = 0;
-    for (size_t p = h + 1; p < e && bases < k; ++p) {
-      char c = d[p];
-      if (c == '\n' || c == '\r') continue;
-      w[bases >> 4] |= (uint32_t)kLut.code[(uint8_t)c] << (2 * (bases & 15));
+    size_t p = h + 1;
+    const uint8_t *code = kLut.code;
+    while (bases < k && p < e) {
+      if (bases + 16 <= k && p + 16 <= e) {
+        const uint8_t *q = (const uint8_t *)d + p;
+        uint32_t v = 0;
+        uint8_t any = 0;
+#pragma GCC unroll 16
+        for (int j = 0; j < 16; ++j) {
+          uint8_t c = code[q[j]];
+          any |= c;
+          v |= (uint32_t)(c & 3) << (2 * j);
+        }
+        if (!(any & kSkip)) {
+          int wi = bases >> 4, sh = 2 * (bases & 15);
+          w[wi] |= v << sh;
+          if (sh) w[wi + 1] |= v >> (32 - sh);
+          bases += 16;
+          p += 16;
+          continue;
+        }
+      }
+      uint8_t c = code[(uint8_t)d[p++]];
+      if (c & kSkip) continue;
+      w[bases >> 4] |= (uint32_t)c << (2 * (bases & 15));
       ++bases;
     }
     if (bases >= k) {
@@ -147,6 +172,7 @@ extern "C" int r2m_fasta_reads(const char *data, size_t len, int k, int nthreads
     size_t off = 0;
     for (size_t j = 0; j < p.hlen.size(); ++j) {
       r->heads.append(p.heads, off, p.hlen[j]);
+      r->heads.push_back('\n');
       off += p.hlen[j];
       r->hoff.push_back(r->heads.size());
     }
@@ -169,8 +195,17 @@ extern "C" const char *r2m_reads_header(const r2m_reads *r, int64_t i, size_t *l
     if (len) *len = 0;
     return nullptr;
   }
-  if (len) *len = r->hoff[i + 1] - r->hoff[i];
+  if (len) *len = r->hoff[i + 1] - r->hoff[i] - 1;
   return r->heads.data() + r->hoff[i];
+}
+
+extern "C" const char *r2m_reads_header_blob(const r2m_reads *r, size_t *total_len) {
+  if (total_len) *total_len = r ? r->heads.size() : 0;
+  return r ? r->heads.data() : nullptr;
+}
+
+extern "C" const size_t *r2m_reads_header_offsets(const r2m_reads *r) {
+  return r ? r->hoff.data() : nullptr;
 }
 
 extern "C" void r2m_reads_free(r2m_reads *r) { delete r; }

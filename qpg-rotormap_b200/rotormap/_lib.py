@@ -64,7 +64,15 @@ SIGNATURES = [
     ("r2m_reads_count", I64, [P]),
     ("r2m_reads_words", P, [P]),
     ("r2m_reads_header", P, [P, I64, ctypes.POINTER(SZ)]),
+    ("r2m_reads_header_blob", P, [P, ctypes.POINTER(SZ)]),
+    ("r2m_reads_header_offsets", P, [P]),
     ("r2m_reads_free", None, [P]),
+    ("r2m_fasta_reads_device", I, [P, SZ, I, P, ctypes.POINTER(P)]),
+    ("r2m_dreads_count", I64, [P]),
+    ("r2m_dreads_words", P, [P]),
+    ("r2m_dreads_spans", P, [P]),
+    ("r2m_dreads_header_blob", P, [P, ctypes.POINTER(SZ)]),
+    ("r2m_dreads_free", None, [P]),
 ]
 
 _lib = None

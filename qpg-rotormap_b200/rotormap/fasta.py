@@ -1,7 +1,9 @@
 """FASTA reads -> forward 2-bit words (mirror of RotorMap/fasta/reader.jl).
 
-Parsing runs in the library's native C++ reader (r2m_fasta_reads); this
-module only moves its result into numpy.
+Two readers with the same result: fasta_reads parses on the host in the
+library's native C++ reader (r2m_fasta_reads) and returns numpy words;
+fasta_reads_device uploads the FASTA bytes and parses them on the GPU
+(r2m_fasta_reads_device), leaving the words in HBM for the encoder.
 """
 from __future__ import annotations
 
@@ -12,7 +14,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import check, lib, ptr, require_device, stream_handle
 
 
 @dataclass
@@ -46,9 +48,11 @@ def fasta_reads(src, k: int = 20_000, parts: int | None = None) -> FastaFragment
         raise ValueError("k must be >= 1")
     data = _read_bytes(src)
     n = len(data)
+    keep = None
     if isinstance(data, mmap.mmap):
-        buf = (ctypes.c_char * n).from_buffer_copy(data) if n else b""
-        data.close()
+        # parse straight from the mapping (no copy of the file)
+        keep = np.frombuffer(data, np.uint8)
+        buf = ctypes.c_char_p(keep.ctypes.data)
     else:
         buf = data
     handle = ctypes.c_void_p()
@@ -65,10 +69,109 @@ def fasta_reads(src, k: int = 20_000, parts: int | None = None) -> FastaFragment
         else:
             words = np.zeros((0, W), np.uint32)
         heads = []
-        ln = ctypes.c_size_t()
-        for i in range(cnt):
-            p = L.r2m_reads_header(handle, i, ctypes.byref(ln))
-            heads.append(ctypes.string_at(p, ln.value).decode("latin-1"))
+        if cnt:
+            tot = ctypes.c_size_t()
+            bp = L.r2m_reads_header_blob(handle, ctypes.byref(tot))
+            # every header is followed by one '\n' and contains none
+            heads = ctypes.string_at(bp, tot.value).decode("latin-1").split("\n")[:cnt]
     finally:
         L.r2m_reads_free(handle)
+        if keep is not None:
+            del keep
+            data.close()
     return FastaFragments(k, words, heads)
+
+
+@dataclass
+class DeviceFastaFragments:
+    """Kept records parsed on the GPU: words (n, cld(k,16)) int32 on the
+    device (the uint32 bit pattern), verbatim '>' headers on the host."""
+    k: int
+    words: "torch.Tensor"
+    heads: list
+
+    def __len__(self) -> int:
+        return len(self.heads)
+
+
+_PINNED: dict = {}
+
+
+def _pinned(tag: str, nbytes: int):
+    """A grow-only pinned host buffer per tag (callers synchronise before reuse)."""
+    import torch
+    buf = _PINNED.get(tag)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, pin_memory=True)
+        _PINNED[tag] = buf
+    return buf[:nbytes]
+
+
+def fasta_reads_device(src, k: int = 20_000, device=None, stream=None) -> DeviceFastaFragments:
+    """fasta_reads on the GPU: the same records, words and headers.
+
+    src is FASTA bytes, a path, or a uint8 CUDA tensor already holding the
+    bytes.  Host sources are staged through a reused pinned buffer and
+    copied to the device on `stream`; the parse runs there; the headers come
+    back as one blob ('\n' after each) and are split on the host.
+    """
+    import torch
+
+    if k < 1:
+        raise ValueError("k must be >= 1")
+    require_device()
+    if isinstance(src, torch.Tensor):
+        if not src.is_cuda or src.dtype != torch.uint8:
+            raise ValueError("a tensor source must be a uint8 CUDA tensor")
+        dev_bytes = src.contiguous().view(-1)
+        dev = dev_bytes.device
+        host = None
+    else:
+        data = _read_bytes(src)
+        host = np.frombuffer(data, np.uint8) if len(data) else np.zeros(0, np.uint8)
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        dev_bytes = None
+    st = stream if stream is not None else torch.cuda.current_stream(dev)
+    L = lib()
+    with torch.cuda.device(dev), torch.cuda.stream(st):
+        if dev_bytes is None:
+            stage = _pinned("fasta_in", host.size)
+            if host.size:
+                stage.numpy()[:] = host
+            dev_bytes = stage.to(dev, non_blocking=True)
+        handle = ctypes.c_void_p()
+        n = int(dev_bytes.numel())
+        check(L.r2m_fasta_reads_device(ptr(dev_bytes) if n else None, n, k, stream_handle(st), ctypes.byref(handle)))
+        try:
+            cnt = int(L.r2m_dreads_count(handle))
+            W = (k + 15) // 16
+            words = torch.empty((cnt, W), dtype=torch.int32, device=dev)
+            heads = []
+            if cnt:
+                words.view(-1).copy_(_wrap_device(L.r2m_dreads_words(handle), cnt * W, torch.int32, dev))
+                tot = ctypes.c_size_t()
+                hp = L.r2m_dreads_header_blob(handle, ctypes.byref(tot))
+                hb = _pinned("fasta_heads", tot.value)
+                hb.copy_(_wrap_device(hp, tot.value, torch.uint8, dev), non_blocking=True)
+                st.synchronize()
+                heads = hb.numpy().tobytes().decode("latin-1").split("\n")[:cnt]
+        finally:
+            st.synchronize()
+            L.r2m_dreads_free(handle)
+    return DeviceFastaFragments(k, words, heads)
+
+
+def _wrap_device(addr: int, count: int, dtype, dev):
+    """A torch view of `count` elements of library-owned device memory."""
+    import torch
+
+    class _Cai:
+        __cuda_array_interface__ = {
+            "shape": (count,),
+            "typestr": {torch.int32: "<i4", torch.int64: "<i8", torch.uint8: "|u1"}[dtype],
+            "data": (addr, False),
+            "version": 3,
+            "strides": None,
+        }
+
+    return torch.as_tensor(_Cai(), device=dev)

@@ -67,6 +67,31 @@ def test_fasta_reader_matches_oracle(ci, k):
         assert got.words.shape[0] == 0
 
 
+@pytest.mark.parametrize("seed", range(6))
+def test_fasta_reader_random_layouts_match_oracle(seed):
+    """Random line widths, LF/CRLF/CR line ends, lower case and non-ACGT bytes:
+    the reader's 16-byte packing steps straddle every kind of line break."""
+    rng = np.random.default_rng(seed)
+    alphabet = np.frombuffer(b"ACGTacgtNRYn-*", np.uint8)
+    out = [b"preamble\n"] if seed % 2 else []
+    for r in range(40):
+        n = int(rng.integers(0, 300))
+        w = np.r_[[0.22] * 4, [0.02] * 4, [0.01] * 6]
+        seq = alphabet[rng.choice(alphabet.size, n, p=w / w.sum() if seed % 3 else None)]
+        eol = [b"\n", b"\r\n", b"\r"][int(rng.integers(0, 3))] if seed >= 3 else b"\n"
+        width = int(rng.integers(1, 90))
+        body = eol.join(seq[i:i + width].tobytes() for i in range(0, n, width))
+        hdr_eol = b"\r\n" if eol == b"\r\n" else b"\n"
+        out.append(b">rec%d %d" % (r, n) + hdr_eol + body + eol)
+    raw = b"".join(out)
+    for k in (1, 15, 16, 17, 48, 150):
+        got = rm.fasta_reads(raw, k=k, parts=1)
+        ref = orc.fasta_reads_ref(raw, k)
+        assert got.heads == [h for h, _ in ref]
+        if ref:
+            assert np.array_equal(got.words, np.stack([w for _, w in ref]))
+
+
 def test_fasta_reader_threads_do_not_change_the_result():
     recs = synth.random_genome([1000] * 6000, seed=9)
     heads = [f">rec_{i} x" for i in range(6000)]
