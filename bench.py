@@ -429,6 +429,61 @@ def batching_leg(dev, n_requests: int, seed: int = 61):
     return out
 
 
+def fasta_leg(dev, n_reads: int = 400_000, seed: int = 71):
+    """Reads-side FASTA parsing: the native host reader (all cores) against
+    the GPU reader, on a FASTA of n_reads 150 bp reads with provenance-style
+    headers.  Device figures: the C entry on bytes already in HBM (CUDA
+    events, 5 calls) and the Python API from host bytes (H2D of the file,
+    the parse, words left on the device, headers back to the host)."""
+    import ctypes
+
+    import torch
+
+    import rotormap as rm
+    from rotormap import synth
+    from rotormap._lib import check, lib, ptr, stream_handle
+    rng = np.random.default_rng(seed)
+    codes = rng.integers(0, 4, (n_reads, K_BASES), dtype=np.uint8)
+    pos = rng.integers(1, 100_000_000, n_reads)
+    letters = synth.LETTERS[codes]
+    raw = b"".join(b">read_%d start=%d len=150 src=chr1\n" % (i, pos[i]) + letters[i].tobytes() + b"\n"
+                   for i in range(n_reads))
+    nbytes = len(raw)
+    threads = os.cpu_count() or 1
+    rm.fasta_reads(raw, k=K_BASES, parts=threads)
+    t0 = time.perf_counter()
+    h = rm.fasta_reads(raw, k=K_BASES, parts=threads)
+    t_host = time.perf_counter() - t0
+    d_raw = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
+    for _ in range(3):
+        g = rm.fasta_reads_device(raw, k=K_BASES, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = rm.fasta_reads_device(raw, k=K_BASES, device=dev)
+    torch.cuda.synchronize()
+    t_api = time.perf_counter() - t0
+    same = g.heads == h.heads and np.array_equal(g.words.cpu().numpy().view(np.uint32), h.words)
+    L = lib()
+    hd = ctypes.c_void_p()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(5):
+        check(L.r2m_fasta_reads_device(ptr(d_raw), nbytes, K_BASES, stream_handle(st), ctypes.byref(hd)))
+        L.r2m_dreads_free(hd)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    del d_raw, g
+    torch.cuda.empty_cache()
+    return {"workload": f"{n_reads} reads of 150 bp, {nbytes} bytes of FASTA", "bytes": nbytes,
+            "host_native_s": t_host, "host_native_GBps": nbytes / t_host / 1e9, "host_threads": threads,
+            "device_c_entry_ms": ms, "device_c_entry_GBps": nbytes / ms / 1e6,
+            "device_api_from_host_s": t_api, "device_api_from_host_GBps": nbytes / t_api / 1e9,
+            "identical_to_host_reader": bool(same)}
+
+
 # ---------------------------------------------------------------- GPU leg
 
 
@@ -446,6 +501,7 @@ def main():
     ap.add_argument("--requests", type=int, default=16, help="requests in the serving leg")
     ap.add_argument("--no-precision", action="store_true", help="skip the precision leg")
     ap.add_argument("--no-batching", action="store_true", help="skip the batching leg")
+    ap.add_argument("--no-fasta", action="store_true", help="skip the FASTA reader leg")
     ap.add_argument("--batching-requests", type=int, default=48)
     ap.add_argument("--precision-reads", type=int, default=100_000)
     ap.add_argument("--precision-sample", type=int, default=1000)
@@ -589,6 +645,8 @@ def main():
             line["precision"] = precision_leg(dev, args.precision_reads, args.precision_sample)
         if world == 1 and not args.no_batching:
             line["batching"] = batching_leg(dev, args.batching_requests)
+        if world == 1 and not args.no_fasta:
+            line["fasta_reader"] = fasta_leg(dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

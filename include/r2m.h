@@ -255,6 +255,27 @@ const char *r2m_reads_header_blob(const r2m_reads *r, size_t *total_len);
 const size_t *r2m_reads_header_offsets(const r2m_reads *r);
 void r2m_reads_free(r2m_reads *r);
 
+/* ----------------------------------------------------------- host genome */
+
+typedef struct r2m_genome r2m_genome;
+
+/* Reference-genome FASTA -> packed records for the index builder: the
+ * record walk of build_index_matrix (RotorMap/index/build.jl:291-324) and
+ * the record table of RotorMap/test/harness.jl:52-91 (header to the first
+ * '\n' at or after the record start, one trailing '\r' removed; sequence
+ * bytes up to the next record start, '\n'/'\r' skipped, A/C/G/T either
+ * case -> 0..3, anything else -> 2).  Every record's bases are 2-bit packed
+ * from a word boundary and followed by one zero guard word.  nthreads host
+ * threads. */
+int r2m_fasta_genome(const char *data, size_t len, int nthreads, r2m_genome **out);
+int64_t r2m_genome_count(const r2m_genome *g);
+const uint32_t *r2m_genome_words(const r2m_genome *g, size_t *nwords);
+const int64_t *r2m_genome_word_off(const r2m_genome *g);  /* per record */
+const int64_t *r2m_genome_nbases(const r2m_genome *g);    /* per record */
+/* every header followed by one '\n' (total bytes in *total_len) */
+const char *r2m_genome_header_blob(const r2m_genome *g, size_t *total_len);
+void r2m_genome_free(r2m_genome *g);
+
 /* ---------------------------------------------------------- device FASTA */
 
 typedef struct r2m_dreads r2m_dreads;

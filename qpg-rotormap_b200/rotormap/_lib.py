@@ -67,6 +67,13 @@ SIGNATURES = [
     ("r2m_reads_header_blob", P, [P, ctypes.POINTER(SZ)]),
     ("r2m_reads_header_offsets", P, [P]),
     ("r2m_reads_free", None, [P]),
+    ("r2m_fasta_genome", I, [ctypes.c_void_p, SZ, I, ctypes.POINTER(P)]),
+    ("r2m_genome_count", I64, [P]),
+    ("r2m_genome_words", P, [P, ctypes.POINTER(SZ)]),
+    ("r2m_genome_word_off", P, [P]),
+    ("r2m_genome_nbases", P, [P]),
+    ("r2m_genome_header_blob", P, [P, ctypes.POINTER(SZ)]),
+    ("r2m_genome_free", None, [P]),
     ("r2m_fasta_reads_device", I, [P, SZ, I, P, ctypes.POINTER(P)]),
     ("r2m_dreads_count", I64, [P]),
     ("r2m_dreads_words", P, [P]),

@@ -15,7 +15,7 @@ import torch
 from . import _lib
 from ._lib import Tuning, check, lib, ptr, stream_handle
 from .encoder import RopeEncoder, encode_frag_real_batch, f16_to_f8
-from .fasta import FastaFragments, fasta_reads
+from .fasta import DeviceFastaFragments, FastaFragments, fasta_reads, fasta_reads_device
 
 _MODES = {"f16": _lib.SCORE_F16, "f32": _lib.SCORE_F32, "scaled": _lib.SCORE_SCALED}
 # fused kernel variant: one CTA per 128-read tile, or CTA pairs (cta_group::2)
@@ -248,16 +248,17 @@ class Mapper:
 # ------------------------------------------------------------------ flows
 
 
-def _batches(frags: FastaFragments, batch_size: int):
+def _batches(frags: FastaFragments | DeviceFastaFragments, batch_size: int):
     for b0 in range(0, len(frags), batch_size):
         yield b0, frags.words[b0:b0 + batch_size], frags.heads[b0:b0 + batch_size]
 
 
 def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stream=None):
     """topk_flow (engine_fp8.jl:498-547) over an iterable of
-    (first0, words (nb, W) uint32, heads) batches: encode on the GPU straight
-    to e4m3 (fp16-rounded, or per-row scaled for score = "scaled"), search,
-    and yield TopKBatch with host arrays."""
+    (first0, words (nb, W), heads) batches -- words as host uint32 arrays or
+    as int32 CUDA tensors already on the engine's device: encode on the GPU
+    straight to e4m3 (fp16-rounded, or per-row scaled for score = "scaled"),
+    search, and yield TopKBatch with host arrays."""
     dev = eng.B.device
     st = stream if stream is not None else torch.cuda.current_stream(dev)
     scaled = eng.score == "scaled"
@@ -267,9 +268,14 @@ def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stre
             continue
         if nb > eng.rows_cap:
             raise ValueError(f"batch height {nb} > engine rows_cap {eng.rows_cap}")
-        hw = torch.from_numpy(np.ascontiguousarray(words, dtype=np.uint32)).pin_memory()
+        on_device = isinstance(words, torch.Tensor) and words.is_cuda
+        if not on_device:
+            hw = torch.from_numpy(np.ascontiguousarray(words, dtype=np.uint32)).pin_memory()
         with torch.cuda.stream(st):
-            dw = hw.to(dev, non_blocking=True).view(torch.int32)
+            if on_device:
+                dw = words.contiguous()
+            else:
+                dw = hw.to(dev, non_blocking=True).view(torch.int32)
             norms = torch.empty((nb, re.m), dtype=torch.float32, device=dev)
             a8 = eng.a8[:nb]
             sa = eng.scaleA[:nb] if scaled else None
@@ -285,12 +291,22 @@ def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stre
 def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int | None = None,
                      batch_size: int = 8192, rows_cap: int | None = None, normalize: int = 0,
                      score: str = "f16", scaleB: torch.Tensor | None = None, parts: int | None = None,
-                     segs: int | None = None, engine: TopKEngine | None = None, stream=None):
+                     segs: int | None = None, engine: TopKEngine | None = None, stream=None,
+                     reader: str = "device"):
     """rope_topk_stream (engine_fp8.jl:576-594): FASTA -> encode -> fp8 GEMM +
-    top-k against the resident B -> TopKBatch per batch (file order)."""
+    top-k against the resident B -> TopKBatch per batch (file order).
+
+    reader = "device" parses the FASTA on the GPU (the words stay in HBM);
+    "host" uses the native host reader with `parts` threads.  Both give the
+    same reads."""
     if B.shape[1] != re.rdim:
         raise ValueError(f"B is {tuple(B.shape)}; the encoder's real embedding dim is {re.rdim}")
-    frags = fasta_reads(file, k=re.k, parts=parts)
+    if reader == "device":
+        frags = fasta_reads_device(file, k=re.k, device=B.device, stream=stream)
+    elif reader == "host":
+        frags = fasta_reads(file, k=re.k, parts=parts)
+    else:
+        raise ValueError('reader must be "device" or "host"')
     eng = engine or TopKEngine(B, k=k, rows_cap=rows_cap or batch_size, score=score, scaleB=scaleB)
     yield from topk_flow(_batches(frags, batch_size), eng, re, normalize, stream)
 

@@ -33,11 +33,6 @@ FP8_FORMAT = "indexreal.fp8.v1"          # load.jl:31
 SCALED_FORMAT = "indexreal.fp8scaled.v1"  # per-column scaled e4m3 (precision form)
 _MAGIC = b"R2MIDX01"
 
-_LUT = np.full(256, 2, dtype=np.uint8)  # reader.jl:21-28: junk / IUPAC -> G
-for _ch, _code in (("A", 0), ("C", 1), ("G", 2), ("T", 3), ("a", 0), ("c", 1), ("g", 2), ("t", 3)):
-    _LUT[ord(_ch)] = _code
-
-
 @dataclass
 class RefPack:
     """Packed reference: verbatim headers, per-record word offset / base count."""
@@ -72,37 +67,52 @@ def pack_records(heads, codes_list) -> RefPack:
     return RefPack(list(heads), np.array(offs, np.int64), np.array(nb, np.int64), words)
 
 
-def _record_spans(raw: bytes):
-    """(start, header_end, seq_lo, seq_hi) per record (build.jl:291-324 walk)."""
-    arr = np.frombuffer(raw, np.uint8)
-    n = arr.size
-    gt = np.flatnonzero(arr == 0x3E)
-    if gt.size:
-        prev = np.where(gt > 0, arr[np.maximum(gt - 1, 0)], 0x0A)
-        gt = gt[(gt == 0) | (prev == 0x0A) | (prev == 0x0D)]
-    nls = np.flatnonzero(arr == 0x0A)
-    spans = []
-    for i, s in enumerate(gt):
-        e = gt[i + 1] if i + 1 < gt.size else n
-        j = np.searchsorted(nls, s)
-        h = nls[j] if j < nls.size else n  # header line ends at the first '\n' (any later)
-        hend = h
-        if hend > s and arr[hend - 1] == 0x0D:
-            hend -= 1
-        spans.append((int(s), int(hend), int(h) + 1, int(e)))
-    return arr, spans
-
-
-def pack_reference(raw: bytes) -> RefPack:
-    """Parse a reference FASTA (bytes) and pack every record."""
-    arr, spans = _record_spans(raw)
-    heads, codes_list = [], []
-    for s, hend, lo, hi in spans:
-        heads.append(bytes(arr[s:hend]).decode("latin-1"))
-        body = arr[lo:hi] if lo < hi else arr[0:0]
-        body = body[(body != 0x0A) & (body != 0x0D)]
-        codes_list.append(_LUT[body])
-    return pack_records(heads, codes_list)
+def pack_reference(src, nthreads: int | None = None) -> RefPack:
+    """Parse a reference FASTA (bytes or a path) and pack every record, in
+    the library's native multithreaded packer (r2m_fasta_genome; the record
+    walk of build.jl:291-324)."""
+    import ctypes
+    import mmap
+    if isinstance(src, (bytes, bytearray, memoryview)):
+        data, keep = bytes(src), None
+    else:
+        path = os.fspath(src)
+        if os.path.getsize(path) == 0:
+            data, keep = b"", None
+        else:
+            with open(path, "rb") as f:
+                keep = mmap.mmap(f.fileno(), 0, access=mmap.ACCESS_READ)
+            data = None
+    L = lib()
+    handle = ctypes.c_void_p()
+    if keep is not None:
+        arr = np.frombuffer(keep, np.uint8)
+        addr, n = arr.ctypes.data, arr.size
+    else:
+        arr = np.frombuffer(data, np.uint8) if data else np.zeros(0, np.uint8)
+        addr, n = (arr.ctypes.data if arr.size else None), arr.size
+    try:
+        check(L.r2m_fasta_genome(addr, n, nthreads or (os.cpu_count() or 1), ctypes.byref(handle)))
+    finally:
+        del arr
+        if keep is not None:
+            keep.close()
+    try:
+        R = int(L.r2m_genome_count(handle))
+        nw = ctypes.c_size_t()
+        wp = L.r2m_genome_words(handle, ctypes.byref(nw))
+        words = np.ctypeslib.as_array((ctypes.c_uint32 * nw.value).from_address(wp)).copy()
+        if R:
+            off = np.ctypeslib.as_array((ctypes.c_int64 * R).from_address(L.r2m_genome_word_off(handle))).copy()
+            nb = np.ctypeslib.as_array((ctypes.c_int64 * R).from_address(L.r2m_genome_nbases(handle))).copy()
+            tot = ctypes.c_size_t()
+            hp = L.r2m_genome_header_blob(handle, ctypes.byref(tot))
+            heads = ctypes.string_at(hp, tot.value).decode("latin-1").split("\n")[:R]
+        else:
+            off, nb, heads = np.zeros(0, np.int64), np.zeros(0, np.int64), []
+    finally:
+        L.r2m_genome_free(handle)
+    return RefPack(heads, off, nb, words)
 
 
 def window_positions(pack: RefPack, k: int, kstep: int):
@@ -202,8 +212,7 @@ def build_index(re: RopeEncoder, source, kstep: int | None = None, batch_size: i
         raise ValueError("kstep and batch_size must be >= 1")
     _lib.require_device()
     if pack is None:
-        raw = source if isinstance(source, (bytes, bytearray)) else open(source, "rb").read()
-        pack = pack_reference(bytes(raw))
+        pack = pack_reference(source)
         src_name = "<bytes>" if isinstance(source, (bytes, bytearray)) else os.path.abspath(source)
     else:
         src_name = str(source)

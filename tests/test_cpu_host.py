@@ -106,6 +106,56 @@ def test_fasta_reader_threads_do_not_change_the_result():
     assert np.array_equal(np.stack([w for _, w in ref]), a.words[:len(ref)])
 
 
+def _unpack(words: np.ndarray, nb: int) -> np.ndarray:
+    return ((words[:, None] >> (2 * np.arange(16, dtype=np.uint32))) & 3).astype(np.uint8).reshape(-1)[:nb]
+
+
+GENOME_CASES = [
+    b"",
+    b"no record\nACGT\n",
+    b"junk\n>chr1 first\nACGTNacgtRYK\nTTTT\n>chr2\r\nGGGGCCCC\r\nAA\r\n>empty\n>last no newline\nACG",
+    b">a\nACGT\r>b run-on header\nCCCC\n>c\nTT>G\n",      # '\r>' starts b inside a's sequence
+    b">h1 header runs on\r>h2\nACGTACGT\n>h3\n" + b"A" * 33 + b"\n",  # h1's '\n' lies in h2
+    b">only header",
+]
+
+
+@pytest.mark.parametrize("ci", range(len(GENOME_CASES)))
+def test_genome_packer_matches_oracle(ci):
+    raw = GENOME_CASES[ci]
+    pack = rm.pack_reference(raw, nthreads=3)
+    heads, seqs = orc.ref_table(raw)
+    assert pack.heads == heads
+    assert list(pack.nbases) == [len(q) for q in seqs]
+    off = 0
+    for r, q in enumerate(seqs):
+        assert pack.word_off[r] == off
+        nw = (len(q) + 15) // 16
+        assert np.array_equal(pack.words[off:off + nw], orc.forward_pack(q, len(q)))
+        assert pack.words[off + nw] == 0  # guard word
+        off += nw + 1
+    assert pack.words.size == max(off, 1)
+
+
+def test_genome_packer_large_records_across_items_and_threads(tmp_path):
+    """Records longer than the packer's 8 MB work items, odd line widths and
+    CRLF: items split mid-record at every base alignment; the result does
+    not depend on the thread count; a path source is read through mmap."""
+    recs = synth.random_genome([21_000_000, 777, 9_000_001], seed=13, n_frac=0.02, run_min=10, run_max=5000)
+    raw = synth.genome_fasta([">big one", ">small", ">mid"], recs, width=61)
+    raw = raw.replace(b"\n", b"\r\n", 200_000)
+    p = tmp_path / "g.fa"
+    p.write_bytes(raw)
+    a = rm.pack_reference(raw, nthreads=1)
+    b = rm.pack_reference(str(p), nthreads=7)
+    assert a.heads == b.heads == [">big one", ">small", ">mid"]
+    assert np.array_equal(a.words, b.words) and np.array_equal(a.word_off, b.word_off)
+    heads, seqs = orc.ref_table(raw)
+    for r, q in enumerate(seqs):
+        assert a.nbases[r] == len(q)
+        assert np.array_equal(_unpack(a.words[a.word_off[r]:], len(q)), q)
+
+
 def test_reference_windows_match_oracle():
     recs = synth.random_genome([700, 149, 150, 333, 2000], seed=4, n_frac=0.1, run_min=5, run_max=40)
     heads = [">A one", ">B", ">C", ">D", ">E"]

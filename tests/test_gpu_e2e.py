@@ -86,6 +86,22 @@ def test_flow_topk_equals_oracle_brute_force(fixture, tmp_path):
         np.testing.assert_allclose(sc[locs[r] - 1], vals[r], atol=1e-3, rtol=0)
 
 
+def test_stream_device_and_host_readers_agree(fixture, tmp_path):
+    """rope_topk_stream with the GPU FASTA reader and with the host reader:
+    the same batches, headers, scores and locations."""
+    heads, recs, re, idx = fixture
+    p, _, hd = _reads_file(tmp_path, heads, recs, 300, 0.05, 13, "rd.fa")
+    a = list(rm.rope_topk_stream(re, str(p), idx.embeds8, k=20, batch_size=128, reader="device"))
+    b = list(rm.rope_topk_stream(re, str(p), idx.embeds8, k=20, batch_size=128, reader="host"))
+    assert [x.heads for x in a] == [x.heads for x in b] and [h for x in a for h in x.heads] == hd
+    for x, y in zip(a, b):
+        assert x.first == y.first
+        assert np.array_equal(x.vals, y.vals) and np.array_equal(x.locs, y.locs)
+        assert np.array_equal(x.norms, y.norms)
+    with pytest.raises(ValueError):
+        next(rm.rope_topk_stream(re, str(p), idx.embeds8, reader="other"))
+
+
 def test_run_map_table(fixture, tmp_path):
     heads, recs, re, idx = fixture
     p, _, hd = _reads_file(tmp_path, heads, recs, 50, 0.0, 3, "rm.fa")
