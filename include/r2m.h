@@ -231,6 +231,32 @@ int r2m_plain_batch_gemm_topk(r2m_plain_engine *eng, const uint8_t *d_A,
                               int nb, float *d_vals, int32_t *d_locs,
                               r2m_stream_t stream);
 
+/* ------------------------------------------------------- host-ring engine */
+
+typedef struct r2m_compact r2m_compact;
+
+/* Replaces CompactEngine (RotorMap/search/engine_compact.jl:256-289): the
+ * index h_B (N, rdim) e4m3 stays in HOST memory and is streamed through a
+ * ring of `depth` device slots of about chunk_cols columns on its own H2D
+ * stream.  d_scaleB (scaled scores) is a device vector of N column scales.
+ * pin != 0 page-locks h_B for the engine's lifetime (read-only
+ * registration; left pageable when the system refuses).  The host memory
+ * must stay valid and unchanged while the engine lives. */
+int r2m_compact_create(const uint8_t *h_B, const float *d_scaleB, int rdim, int64_t N, int k, int rows_cap,
+                       int score_mode, int64_t chunk_cols, int depth, int pin, const r2m_tuning *tune,
+                       r2m_compact **out);
+int r2m_compact_destroy(r2m_compact *c);
+int64_t r2m_compact_chunks(const r2m_compact *c);
+int r2m_compact_is_pinned(const r2m_compact *c);
+/* Replaces batch_gemm_topk_compact! (RotorMap/search/engine_compact.jl:
+ * 300-343): the same results as r2m_batch_gemm_topk over the whole index
+ * (values, locations and tie order, bit for bit).  Enqueues on `stream`
+ * (chunk copies on the engine's H2D stream, ordered by events) and returns;
+ * with a pageable h_B each chunk copy holds the host until the slot it
+ * refills is free. */
+int r2m_compact_batch_gemm_topk(r2m_compact *c, const uint8_t *d_A, const float *d_scaleA, int nb,
+                                float *d_vals, int32_t *d_locs, r2m_stream_t stream);
+
 /* ------------------------------------------------------------ host FASTA */
 
 typedef struct r2m_reads r2m_reads;

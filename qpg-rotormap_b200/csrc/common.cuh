@@ -35,6 +35,9 @@ inline cudaStream_t as_stream(r2m_stream_t s) { return (cudaStream_t)s; }
 
 // Number of SMs of the current device (cached per device).
 int sm_count();
+// Re-point an engine (gemm_topk.cu) at another B of at most its creation
+// column count; used by the host-ring engine for each ring slot.
+int engine_rebind(::r2m_engine *eng, const uint8_t *d_B, const float *d_scaleB, int64_t N);
 // Stream-ordered allocation from the library's per-device pool (freed with
 // cudaFreeAsync); the pool keeps up to 1 GiB mapped between calls.
 cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t st);

@@ -848,6 +848,7 @@ struct r2m_engine {
   const float *scaleB;
   int rdim;
   long long N;
+  long long N_cap;  // columns at creation (the workspace is sized for them)
   int k, KT;
   int rows_cap;
   int score_mode;
@@ -888,6 +889,7 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   e->scaleB = d_scaleB;
   e->rdim = rdim;
   e->N = N;
+  e->N_cap = N;
   e->k = k;
   e->KT = pick_kt(k);
   e->rows_cap = rows_cap;
@@ -972,6 +974,31 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   eng->mode = mode;
   return R2M_OK;
 }
+
+namespace r2m {
+// Point the engine at another B (and scaleB) of at most the columns it was
+// created for: the split workspace stays valid, the tensor maps are encoded
+// again on the host.  The maps reach the kernels as launch parameters, so
+// launches already queued keep the previous B.
+int engine_rebind(r2m_engine *eng, const uint8_t *d_B, const float *d_scaleB, int64_t N) {
+  R2M_REQUIRE(eng != nullptr && d_B != nullptr, "null pointer");
+  R2M_REQUIRE(N >= eng->k && N <= eng->N_cap, "rebind: N must be in k..N at creation");
+  R2M_REQUIRE((reinterpret_cast<uintptr_t>(d_B) & 15) == 0, "B must be 16-byte aligned");
+  R2M_REQUIRE(eng->score_mode != R2M_SCORE_SCALED || (d_scaleB && (reinterpret_cast<uintptr_t>(d_scaleB) & 15) == 0),
+              "scaled scores need a 16-byte aligned scaleB");
+  CUtensorMap m, m128;
+  int rc = make_map(&m, d_B, N, eng->rdim, BN);
+  if (!rc) rc = make_map(&m128, d_B, N, eng->rdim, 128);
+  if (rc) return rc;
+  eng->B = d_B;
+  eng->scaleB = d_scaleB;
+  eng->N = N;
+  eng->n_tiles = (int)((N + BN - 1) / BN);
+  eng->mapB = m;
+  eng->mapB128 = m128;
+  return R2M_OK;
+}
+}  // namespace r2m
 
 extern "C" int64_t r2m_engine_workspace_bytes(const r2m_engine *eng) {
   if (!eng) return 0;

@@ -7,7 +7,7 @@ librotormap_b200.so (C ABI: include/r2m.h).  There is no CPU fallback.
 from ._lib import R2MError, lib, require_device
 from .encoder import (RopeEncoder, dim, encode_frag_real_batch, encode_frag_real_batch_alloc,
                       f16_to_f8, f32_to_f8, revcomp_frag_words)
-from .engine import (Mapper, PlainEngine, TopKBatch, TopKEngine, batch_gemm_topk, padmul, resident_fits,
+from .engine import (CompactEngine, Mapper, PlainEngine, TopKBatch, TopKEngine, batch_gemm_topk, padmul, resident_fits,
                      rope_topk_stream, rope_topk_stream_compact, topk_flow, upload_fp16_as_f8)
 from .fasta import DeviceFastaFragments, FastaFragments, fasta_reads, fasta_reads_device
 from .index import (FP8_FORMAT, SCALED_FORMAT, Index, RefPack, build_index, build_index_packed,

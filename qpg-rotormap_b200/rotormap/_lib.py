@@ -67,6 +67,11 @@ SIGNATURES = [
     ("r2m_reads_header_blob", P, [P, ctypes.POINTER(SZ)]),
     ("r2m_reads_header_offsets", P, [P]),
     ("r2m_reads_free", None, [P]),
+    ("r2m_compact_create", I, [P, P, I, I64, I, I, I, I64, I, I, P, ctypes.POINTER(P)]),
+    ("r2m_compact_destroy", I, [P]),
+    ("r2m_compact_chunks", I64, [P]),
+    ("r2m_compact_is_pinned", I, [P]),
+    ("r2m_compact_batch_gemm_topk", I, [P, P, P, I, P, P, P]),
     ("r2m_fasta_genome", I, [ctypes.c_void_p, SZ, I, ctypes.POINTER(P)]),
     ("r2m_genome_count", I64, [P]),
     ("r2m_genome_words", P, [P, ctypes.POINTER(SZ)]),

@@ -70,8 +70,8 @@ class Autotuner:
             s, c = self.cache[k]
             eng.set_tuning(s, c)
             return s, c
-        sms = torch.cuda.get_device_properties(eng.B.device).multi_processor_count
-        st = stream or torch.cuda.current_stream(eng.B.device)
+        sms = torch.cuda.get_device_properties(eng.device).multi_processor_count
+        st = stream or torch.cuda.current_stream(eng.device)
         target = eng
         if 0 < self.proxy_cols < eng.N:
             from .engine import TopKEngine
@@ -111,7 +111,7 @@ class RaggedBatcher:
         self.cap = bucket_rows(capacity)
         if self.cap > eng.rows_cap:
             raise ValueError("engine rows_cap must be a multiple of 128 at least the capacity")
-        dev = eng.B.device
+        dev = eng.device
         W, k = re.words, eng.k
         self.h_words = torch.zeros((self.cap, W), dtype=torch.int32, pin_memory=True)
         self.h_vals = torch.empty((self.cap, k), dtype=torch.float32, pin_memory=True)

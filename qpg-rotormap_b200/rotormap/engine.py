@@ -80,6 +80,10 @@ class TopKEngine:
                                       ctypes.byref(tune), ctypes.byref(h)))
         self._h = h
 
+    @property
+    def device(self) -> torch.device:
+        return self.B.device
+
     def set_tuning(self, splits: int = 0, ctas: int = 0, kernel: str | None = None) -> None:
         """Change the schedule (0 = automatic).  Not during stream capture."""
         kernel = kernel or self.kernel
@@ -149,6 +153,10 @@ class PlainEngine:
                                             ctypes.byref(h)))
         self._h = h
 
+    @property
+    def device(self) -> torch.device:
+        return self.B.device
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib().r2m_plain_engine_destroy(self._h)
@@ -176,6 +184,100 @@ class PlainEngine:
         return D_val, D_loc
 
 
+class CompactEngine:
+    """CompactEngine(host; k, rows_cap, ...) (engine_compact.jl:256-289): the
+    index stays in host memory -- a C-contiguous (N, rdim) uint8 numpy array
+    (a memory-mapped index file works) or a CPU uint8 tensor -- and each
+    search streams it through `depth` device slots of about `chunk_cols`
+    columns.  Same search() contract and the same results, bit for bit, as
+    TopKEngine over the whole index.  pin page-locks the host index for the
+    engine's lifetime (full-speed DMA; refused registrations stay pageable).
+    scaleB (scaled scores) is uploaded once (4 bytes per column)."""
+
+    def __init__(self, Bh, k: int = 20, rows_cap: int = 8192, score: str = "f16", scaleB=None,
+                 chunk_cols: int = 1 << 20, depth: int = 3, pin: bool = True, device=None, splits: int = 0,
+                 ctas: int = 0, kernel: str = "auto"):
+        _lib.require_device()
+        if isinstance(Bh, torch.Tensor):
+            if Bh.is_cuda or Bh.dtype != torch.uint8 or Bh.dim() != 2:
+                raise ValueError("a tensor host index must be a 2-D uint8 CPU tensor")
+            Bh = Bh.contiguous()
+            addr = Bh.data_ptr()
+        else:
+            Bh = np.asarray(Bh)
+            if Bh.dtype != np.uint8 or Bh.ndim != 2:
+                raise ValueError("the host index must be a 2-D uint8 array")
+            if not Bh.flags.c_contiguous:
+                Bh = np.ascontiguousarray(Bh)
+            addr = Bh.ctypes.data
+        N, rdim = Bh.shape
+        if score not in _MODES:
+            raise ValueError("score must be 'f16', 'f32' or 'scaled'")
+        if kernel not in _KERNELS:
+            raise ValueError("kernel must be 'auto', '1sm' or '2sm'")
+        self.host, self.k, self.rows_cap, self.score = Bh, k, rows_cap, score
+        self.N, self.rdim = int(N), int(rdim)
+        self._device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.scaleB = None
+        if score == "scaled":
+            if scaleB is None:
+                raise ValueError("scaled scores need scaleB")
+            sb = scaleB if isinstance(scaleB, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(scaleB))
+            self.scaleB = sb.to(self._device, torch.float32).contiguous()
+        self.a8 = torch.zeros((rows_cap, rdim), dtype=torch.uint8, device=self._device)
+        self.scaleA = torch.ones((rows_cap,), dtype=torch.float32, device=self._device)
+        tune = Tuning(splits, ctas)
+        tune.reserved[1] = _KERNELS[kernel]
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self._device):
+            check(lib().r2m_compact_create(addr, ptr(self.scaleB), self.rdim, self.N, k, rows_cap, _MODES[score],
+                                           chunk_cols, depth, 1 if pin else 0, ctypes.byref(tune), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def device(self) -> torch.device:
+        return self._device
+
+    @property
+    def chunks(self) -> int:
+        return int(lib().r2m_compact_chunks(self._h))
+
+    @property
+    def pinned(self) -> bool:
+        return bool(lib().r2m_compact_is_pinned(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().r2m_compact_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, A8: torch.Tensor, nb: int | None = None, scaleA: torch.Tensor | None = None,
+               D_val: torch.Tensor | None = None, D_loc: torch.Tensor | None = None, stream=None):
+        """batch_gemm_topk_compact! (engine_compact.jl:300-343): top-k of rows
+        0..nb-1 of A8 against the host index -> (D_val (nb, k), D_loc (nb, k))."""
+        nb = A8.shape[0] if nb is None else nb
+        if nb > self.rows_cap:
+            raise ValueError(f"batch height {nb} > engine rows_cap {self.rows_cap}")
+        if A8.dtype != torch.uint8 or A8.shape[1] != self.rdim or not A8.is_contiguous():
+            raise ValueError("A8 must be a contiguous (nb, rdim) uint8 tensor")
+        if self.score == "scaled" and scaleA is None:
+            raise ValueError("scaled scores need scaleA")
+        dev = self._device
+        if D_val is None:
+            D_val = torch.empty((nb, self.k), dtype=torch.float32, device=dev)
+        if D_loc is None:
+            D_loc = torch.empty((nb, self.k), dtype=torch.int32, device=dev)
+        check(lib().r2m_compact_batch_gemm_topk(self._h, ptr(A8), ptr(scaleA), nb, ptr(D_val), ptr(D_loc),
+                                                stream_handle(stream)))
+        return D_val, D_loc
+
+
 def upload_fp16_as_f8(eng: TopKEngine, embeds, stream=None) -> torch.Tensor:
     """upload_fp16_as_f8! (engine_fp8.jl:355-371): H2D an fp16 (nb, rdim) batch
     and quantise it into the engine staging `a8` rows 0..nb-1."""
@@ -185,7 +287,7 @@ def upload_fp16_as_f8(eng: TopKEngine, embeds, stream=None) -> torch.Tensor:
     nb, rdim = e.shape
     if rdim != eng.rdim or nb > eng.rows_cap:
         raise ValueError("batch shape does not fit the engine staging")
-    d = e.to(eng.B.device, non_blocking=True).contiguous()
+    d = e.to(eng.device, non_blocking=True).contiguous()
     f16_to_f8(eng.a8[:nb], d, stream)
     return eng.a8
 
@@ -208,7 +310,7 @@ class Mapper:
 
     def __init__(self, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stream=None):
         self.eng, self.re, self.normalize = eng, re, normalize
-        dev = eng.B.device
+        dev = eng.device
         cap = eng.rows_cap
         self.stream = stream or torch.cuda.Stream(dev)
         self.h_words = torch.empty((cap, re.words), dtype=torch.int32, pin_memory=True)
@@ -259,7 +361,7 @@ def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stre
     as int32 CUDA tensors already on the engine's device: encode on the GPU
     straight to e4m3 (fp16-rounded, or per-row scaled for score = "scaled"),
     search, and yield TopKBatch with host arrays."""
-    dev = eng.B.device
+    dev = eng.device
     st = stream if stream is not None else torch.cuda.current_stream(dev)
     scaled = eng.score == "scaled"
     for first0, words, heads in source:
@@ -326,24 +428,43 @@ def resident_fits(host_bytes: int, rows_cap: int, rdim: int, k: int = 20, device
 
 def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size: int = 8192,
                              rows_cap: int | None = None, normalize: int = 0, score: str = "f16",
-                             scaleB=None, resident: bool | None = None, **kw):
-    """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index.
-
-    A B200's 180 GB hold every index this path targets, so the auto policy
-    uploads B once (resident); an index that does not fit raises instead of
-    streaming it through a host ring."""
+                             scaleB=None, resident: bool | None = None, chunk_cols: int = 1 << 20,
+                             depth: int = 3, pin: bool = True, reader: str = "device", parts: int | None = None,
+                             stream=None):
+    """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index
+    Bh (N, rdim) uint8.  resident = None applies resident_fits: an index that
+    fits beside the engine's working set is uploaded once and searched by
+    the resident engine; otherwise (or resident = False) it stays in host
+    memory and every batch streams it through the CompactEngine ring.  Both
+    give the same batches."""
     Bh = np.asarray(Bh) if not isinstance(Bh, torch.Tensor) else Bh
     nbytes = Bh.nbytes if isinstance(Bh, np.ndarray) else Bh.numel()
     cap = rows_cap or batch_size
     if resident is None:
         resident = resident_fits(nbytes, cap, re.rdim, k)
-    if not resident:
-        raise MemoryError("index + engine working set exceed free device memory "
-                          "(host-ring streaming is not part of this build)")
-    B = Bh if isinstance(Bh, torch.Tensor) and Bh.is_cuda else torch.from_numpy(np.ascontiguousarray(Bh)).cuda()
     sb = None
     if scaleB is not None:
         sb = scaleB if isinstance(scaleB, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(scaleB))
         sb = sb.cuda()
-    yield from rope_topk_stream(re, file, B, k=k, batch_size=batch_size, rows_cap=cap,
-                                normalize=normalize, score=score, scaleB=sb, **kw)
+    if resident:
+        if isinstance(Bh, torch.Tensor):
+            B = Bh if Bh.is_cuda else Bh.cuda()
+        else:
+            B = torch.from_numpy(np.ascontiguousarray(Bh)).cuda()
+        yield from rope_topk_stream(re, file, B, k=k, batch_size=batch_size, rows_cap=cap, normalize=normalize,
+                                    score=score, scaleB=sb, reader=reader, parts=parts, stream=stream)
+        return
+    if Bh.shape[1] != re.rdim:
+        raise ValueError(f"B is {tuple(Bh.shape)}; the encoder's real embedding dim is {re.rdim}")
+    eng = CompactEngine(Bh, k=k, rows_cap=cap, score=score, scaleB=sb, chunk_cols=chunk_cols, depth=depth,
+                        pin=pin)
+    try:
+        if reader == "device":
+            frags = fasta_reads_device(file, k=re.k, device=eng.device, stream=stream)
+        elif reader == "host":
+            frags = fasta_reads(file, k=re.k, parts=parts)
+        else:
+            raise ValueError('reader must be "device" or "host"')
+        yield from topk_flow(_batches(frags, batch_size), eng, re, normalize, stream)
+    finally:
+        eng.close()

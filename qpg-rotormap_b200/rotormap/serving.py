@@ -69,7 +69,7 @@ class MappingServer:
     def __init__(self, eng, re: RopeEncoder, hbm_budget: int | None = None, normalize: int = 0,
                  max_queued_batches: int = 2):
         self.eng, self.re, self.normalize = eng, re, normalize
-        self.dev = eng.B.device
+        self.dev = eng.device
         self.k = eng.k
         self.cap = eng.rows_cap
         self.scaled = eng.score == "scaled"
@@ -247,7 +247,7 @@ def plain_map(eng, re: RopeEncoder, requests, batch: int = 8192, normalize: int 
     at a time, fixed batches, synchronous per batch -> per-request (vals, locs)
     and completion times.  `requests`: [(t_arrival, words)]; `clock` waits
     until each arrival time (wall-clock replay)."""
-    dev = eng.B.device
+    dev = eng.device
     st = torch.cuda.Stream(dev)
     out = []
     W = re.words

@@ -1,0 +1,121 @@
+"""Host-ring engine (r2m_compact_*, the CompactEngine of
+RotorMap/search/engine_compact.jl:256-343): an index in host memory streamed
+through a device chunk ring gives the resident engine's results bit for bit
+-- values, locations and tie order -- in every score mode."""
+import numpy as np
+import pytest
+import torch
+
+import rotormap as rm
+
+from test_gpu_search import int_e4m3, unit_e4m3
+
+pytestmark = pytest.mark.gpu
+
+
+def resident(A8, B8, k, score="f16", scaleA=None, scaleB=None):
+    B = torch.from_numpy(B8).cuda()
+    sb = torch.from_numpy(scaleB).cuda() if scaleB is not None else None
+    sa = torch.from_numpy(scaleA).cuda() if scaleA is not None else None
+    eng = rm.TopKEngine(B, k=k, rows_cap=A8.shape[0], score=score, scaleB=sb)
+    v, l = eng.search(torch.from_numpy(A8).cuda(), A8.shape[0], sa)
+    out = v.cpu().numpy(), l.cpu().numpy()
+    eng.close()
+    return out
+
+
+def compact(A8, B8, k, score="f16", scaleA=None, scaleB=None, chunk_cols=4096, depth=3, pin=True, repeat=1):
+    eng = rm.CompactEngine(B8, k=k, rows_cap=A8.shape[0], score=score, scaleB=scaleB, chunk_cols=chunk_cols,
+                           depth=depth, pin=pin)
+    A = torch.from_numpy(A8).cuda()
+    sa = torch.from_numpy(scaleA).cuda() if scaleA is not None else None
+    outs = []
+    for _ in range(repeat):
+        v, l = eng.search(A, A8.shape[0], sa)
+        outs.append((v.cpu().numpy(), l.cpu().numpy()))
+    chunks = eng.chunks
+    eng.close()
+    return outs, chunks
+
+
+@pytest.mark.parametrize("score", ["f16", "f32"])
+@pytest.mark.parametrize("nb,N,chunk", [(300, 50_000, 4096), (129, 20_000, 256), (1000, 9_000, 8192),
+                                        (64, 70_001, 65_536)])
+def test_ring_equals_resident_with_ties(score, nb, N, chunk):
+    """Integer-valued scores (exact in every order) with many equal values,
+    and exact duplicate columns placed across chunk boundaries."""
+    rng = np.random.default_rng(nb + N)
+    rdim = 256
+    A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
+    B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
+    for c in list(range(0, N - chunk - 7, max(chunk // 2, 1)))[:40]:
+        B8[c + chunk + 3] = B8[c]  # a later chunk holds the same column
+    v0, l0 = resident(A8, B8, 20, score)
+    outs, chunks = compact(A8, B8, 20, score, chunk_cols=chunk, repeat=2)
+    assert chunks == -(-N // chunk)
+    for v, l in outs:
+        assert np.array_equal(v, v0) and np.array_equal(l, l0)
+
+
+def test_ring_scaled_equals_resident():
+    rng = np.random.default_rng(5)
+    nb, N, rdim = 257, 40_000, 256
+    A8 = unit_e4m3(rng, nb, rdim)
+    B8 = unit_e4m3(rng, N, rdim)
+    sa = rng.uniform(0.5, 2.0, nb).astype(np.float32)
+    sb = rng.uniform(0.5, 2.0, N).astype(np.float32)
+    v0, l0 = resident(A8, B8, 32, "scaled", sa, sb)
+    outs, _ = compact(A8, B8, 32, "scaled", sa, sb, chunk_cols=3000, depth=2, repeat=2)
+    for v, l in outs:
+        assert np.array_equal(v, v0) and np.array_equal(l, l0)
+
+
+@pytest.mark.parametrize("pin", [True, False])
+def test_ring_fixed_slots_and_pageable_host(pin):
+    """chunks <= depth: every chunk keeps its slot across searches; a
+    pageable host index gives the same results as a page-locked one."""
+    rng = np.random.default_rng(9)
+    nb, N, rdim = 200, 10_000, 128
+    A8 = unit_e4m3(rng, nb, rdim)
+    B8 = unit_e4m3(rng, N, rdim)
+    v0, l0 = resident(A8, B8, 20)
+    outs, chunks = compact(A8, B8, 20, chunk_cols=4000, depth=3, pin=pin, repeat=3)
+    assert chunks == 3
+    for v, l in outs:
+        assert np.array_equal(v, v0) and np.array_equal(l, l0)
+
+
+def test_ring_rejects_bad_arguments():
+    B8 = np.zeros((1000, 128), np.uint8)
+    with pytest.raises(rm.R2MError):
+        rm.CompactEngine(B8, k=20, chunk_cols=100)          # chunk_cols < 256
+    with pytest.raises(rm.R2MError):
+        rm.CompactEngine(B8, k=20, depth=1)
+    with pytest.raises(ValueError):
+        rm.CompactEngine(B8, k=20, score="scaled")          # no scaleB
+    eng = rm.CompactEngine(B8, k=20, rows_cap=16, chunk_cols=256)
+    with pytest.raises(ValueError):
+        eng.search(torch.zeros((17, 128), dtype=torch.uint8, device="cuda"))
+    eng.close()
+
+
+def test_compact_stream_ring_equals_resident(tmp_path):
+    """rope_topk_stream_compact: the host ring (resident = False) and the
+    uploaded index (resident = True) yield the same batches."""
+    from rotormap import synth
+    heads = [">c1", ">c2"]
+    recs = synth.random_genome([60_000, 40_000], seed=4)
+    re = rm.RopeEncoder(k=150, s=8, m=4, c=4)
+    idx = rm.build_index(re, synth.genome_fasta(heads, recs), kstep=15, scaled=True)
+    reads, hd, _, _ = synth.sample_reads_even(heads, recs, 300, 150, 0.05, seed=8)
+    p = tmp_path / "r.fa"
+    p.write_bytes(synth.reads_fasta(hd, reads))
+    Bh = idx.embeds8.cpu().numpy()
+    sb = idx.scales.cpu().numpy() if isinstance(idx.scales, torch.Tensor) else np.asarray(idx.scales)
+    a = list(rm.rope_topk_stream_compact(re, str(p), Bh, k=20, batch_size=128, score="scaled", scaleB=sb,
+                                         resident=True))
+    b = list(rm.rope_topk_stream_compact(re, str(p), Bh, k=20, batch_size=128, score="scaled", scaleB=sb,
+                                         resident=False, chunk_cols=2048))
+    assert [x.heads for x in a] == [x.heads for x in b]
+    for x, y in zip(a, b):
+        assert np.array_equal(x.vals, y.vals) and np.array_equal(x.locs, y.locs)
