@@ -94,26 +94,38 @@ def substitute(codes: np.ndarray, err: float, rng) -> np.ndarray:
 
 
 def mutate_edits(codes: np.ndarray, err: float, rng) -> np.ndarray:
-    """The reference's mutate model (dna.jl:120-183): ceil(n*err) edit
-    operations, 1/3 substitutions, 1/3 insertions, 1/3 deletions, the result
-    trimmed / padded back to the original length."""
+    """The reference's `mutate` (RotorMap/common/dna.jl:120-183): n_err =
+    ceil(n*err) edit operations -- n_ins = n_del = floor(n_err/3)
+    insertions and deletions, the other n_sub = n_err - 2*n_ins
+    substitutions -- so the length stays exactly n.
+
+    Positions as the reference draws them (1-based, uniform): substitutions
+    ceil(n*u), sorted, with replacement, each replacing the original base by
+    one of the other three; deletions ceil((n-t)*u) for t = 0.., sorted and
+    made strictly increasing; insertions ceil((n-n_del)*u), sorted, of a
+    uniform base.  Applied in that order -- substitutions, then deletions,
+    then insertions at positions of the shortened sequence (the leaf
+    semantics of RotorMap/common/treearrays.jl's subsat!/deleteat!/
+    insertat!).  The draws come from `rng` (numpy), not Julia's Xoshiro."""
+    codes = np.asarray(codes, np.uint8)
     n = codes.size
-    nops = math.ceil(n * err)
-    seq = list(codes.tolist())
-    for _ in range(nops):
-        op = int(rng.integers(0, 3))
-        if op == 0 and seq:
-            i = int(rng.integers(0, len(seq)))
-            seq[i] = (seq[i] + int(rng.integers(1, 4))) % 4
-        elif op == 1:
-            i = int(rng.integers(0, len(seq) + 1))
-            seq.insert(i, int(rng.integers(0, 4)))
-        elif seq:
-            i = int(rng.integers(0, len(seq)))
-            del seq[i]
-    while len(seq) < n:
-        seq.append(int(rng.integers(0, 4)))
-    return np.array(seq[:n], np.uint8)
+    n_err = int(math.ceil(n * err))
+    n_ins = n_err // 3
+    n_del = n_ins
+    n_sub = n_err - n_ins - n_del
+    if n_err == 0:
+        return codes.copy()
+    out = codes.copy()
+    inds_s = np.sort(np.maximum(np.ceil(n * rng.random(n_sub)).astype(np.int64), 1))
+    out[inds_s - 1] = (codes[inds_s - 1] + rng.integers(1, 4, n_sub)) % 4
+    t = np.arange(n_del, dtype=np.int64)
+    inds_d = np.sort(np.maximum(np.ceil((n - t) * rng.random(n_del)).astype(np.int64), 1))
+    for i in range(1, n_del):
+        inds_d[i] = max(inds_d[i], inds_d[i - 1] + 1)
+    out = np.delete(out, inds_d - 1)
+    inds_i = np.sort(np.maximum(np.ceil((n - n_del) * rng.random(n_ins)).astype(np.int64), 1))
+    out = np.insert(out, inds_i - 1, rng.integers(0, 4, n_ins).astype(np.uint8))
+    return out.astype(np.uint8)
 
 
 def sample_reads_even(heads, recs, n: int, k: int, err: float = 0.0, seed: int = 42,

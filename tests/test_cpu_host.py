@@ -267,3 +267,22 @@ def test_synth_even_sampler_and_packing():
         assert np.array_equal(w[i], orc.forward_pack(reads[i], 150))
     mutated = synth.substitute(np.zeros(100000, np.uint8), 0.05, np.random.default_rng(0))
     assert abs((mutated != 0).mean() - 0.05) < 0.005
+
+
+def test_mutate_edits_follows_the_reference_model():
+    """mutate (RotorMap/common/dna.jl:120-183): ceil(n*err) operations split
+    floor(n_err/3) insertions, as many deletions, the rest substitutions; the
+    length stays n; err = 0 is the identity; a substitution-only count (n_err
+    < 3) changes exactly the drawn positions to other bases."""
+    rng = np.random.default_rng(3)
+    codes = rng.integers(0, 4, 5000).astype(np.uint8)
+    assert np.array_equal(synth.mutate_edits(codes, 0.0, rng), codes)
+    for err in (0.0001, 0.01, 0.1, 0.3, 0.5):
+        out = synth.mutate_edits(codes, err, np.random.default_rng(7))
+        assert out.size == codes.size and out.dtype == np.uint8 and out.max() <= 3
+    out = synth.mutate_edits(codes, 2 / 5000, np.random.default_rng(9))  # n_err = 2: two substitutions
+    diff = np.flatnonzero(out != codes)
+    assert 1 <= diff.size <= 2
+    a = synth.mutate_edits(codes, 0.2, np.random.default_rng(11))
+    b = synth.mutate_edits(codes, 0.2, np.random.default_rng(11))
+    assert np.array_equal(a, b)

@@ -27,6 +27,7 @@ CONFIGS = [
     (37, 5, 1, 3),
     (2001, 5, 1, 4),  # nw > 512: the reference thread recurrence
     (20, 8, 2, 2),
+    (20000, 5, 1, 5),  # the reference's production encoder at the reader's default k
 ]
 
 
@@ -170,3 +171,37 @@ def test_ref_windows_columns_match_oracle():
     assert np.array_equal(idx.embeds8.cpu().numpy(), orc.quantize_parity(got))
     assert np.array_equal(idx.strand, strand)
     assert list(idx.starts) == list(st[col_win])
+
+
+def test_reference_experiment_curves_through_the_gpu_encoder():
+    """The reference's committed experiment outputs (k = 20,000, s5 m1 c5;
+    tests/golden/rope_mutation_sweep_bins.json) reproduced by the GPU
+    encoder's fp32 output: the 500-base rotation anchor of the shift sweep
+    to 1e-4, and mutation-sweep inner products equal to the oracle's fp64
+    ones within 1e-5 (the curve itself is checked against the reference's
+    on the CPU)."""
+    import json
+    from pathlib import Path
+    from rotormap import synth
+    sweep = json.loads((Path(__file__).parent / "golden" / "rope_mutation_sweep_bins.json").read_text())
+    K, S, M, C = 20000, 5, 1, 5
+    re = rm.RopeEncoder(k=K, s=S, m=M, c=C)
+    frag = np.random.default_rng(5).integers(0, 4, K).astype(np.uint8)
+    errs = 0.5 * np.arange(1000) / 999
+    muts = [frag, np.roll(frag, -sweep["shift_anchor"]["shift"])]
+    muts += [synth.mutate_edits(frag, errs[i], np.random.default_rng(i)) for i in range(0, 1000, 50)]
+    words = synth.pack_reads(muts, K)
+    g, _ = _gpu_encode(words, re)
+    o, _ = orc.rope_f64(words, K, S, M, C)
+    D = g.shape[1] // 2
+
+    def ip(a, b):
+        a = a.astype(np.float64)
+        b = b.astype(np.float64)
+        r = a @ b
+        return r, np.hypot(r, a[:D] @ b[D:] - a[D:] @ b[:D])
+
+    sr, sa = ip(g[0], g[1])
+    assert abs(sr - sweep["shift_anchor"]["ip_re"]) < 1e-4 and abs(sa - sweep["shift_anchor"]["ip_abs"]) < 1e-4
+    for j in range(2, len(muts)):
+        assert np.allclose(ip(g[0], g[j]), ip(o[0], o[j]), rtol=0, atol=1e-5)
