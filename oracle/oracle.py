@@ -19,10 +19,12 @@ paths relative to the q4bio-qpg/qpg-rotormap tree):
 C restatements (oracle/rotormap_oracle.c, built by oracle/Makefile):
   rope_f64 / rope_f32 / f32_to_e4m3 / f32_to_f16 / topk_e4m3 / scores_e4m3.
 
-Parity status: "parity unpinned" -- the reference (Julia) cannot run in this
-container and commits no golden outputs; the oracle is pinned by the
-reference's own known-answer properties and hand-derived vectors
-(tests/golden/).
+Parity status: "parity unpinned" in the strict sense -- the reference (Julia)
+cannot run in this container and commits no golden input/output vectors; the
+oracle is pinned by the reference's own known-answer properties, hand-derived
+vectors (tests/golden/), and the reference's committed experiment curves
+(tests/golden/rope_mutation_sweep_bins.json: the shift-sweep anchor matched to
+1e-4, the mutation-sweep curve within the fragment-to-fragment spread).
 """
 from __future__ import annotations
 

@@ -9,8 +9,11 @@
  * golden vectors, so this restatement is pinned by the reference's own
  * known-answer properties (unit energy, window / reverse-complement word
  * identities, e4m3 == host conversion, exact top-k multisets) and by the
- * hand-derived vectors under tests/golden/ -- not by outputs of the
- * reference itself ("parity unpinned" in the strict sense).
+ * hand-derived vectors under tests/golden/, and by curves the reference's
+ * own fp64 encoder produced and committed (its experiment outputs at k =
+ * 20,000, s5 m1 c5: tests/golden/rope_mutation_sweep_bins.json) -- not by
+ * input/output vectors of the reference ("parity unpinned" in the strict
+ * sense).
  *
  * Functions and the reference code each one restates:
  *   orc_rope_frag_f64   _ref_rope_frag / _ref_rope_frag_real
