@@ -370,9 +370,17 @@ __global__ void __launch_bounds__(THREADS, 1)
 // multicast is used anywhere.
 constexpr int STAGES2 = 6;
 constexpr int HALF_TILE = 128 * BK;  // 16 KiB
+// CTA-pair kernel: TMA warp, MMA warp and 4 * H epilogue warps.  With H = 2
+// (KT <= 32) two warps share each TMEM lane quarter, each draining one half
+// (128 columns) of every tile into its own reservoir, so a (read tile, column
+// split) unit leaves two partial lists per row; KT = 64 keeps one warp per
+// quarter (H = 1), whose larger reservoir needs the registers.
+__host__ __device__ constexpr int pair_halves(int KT) { return KT >= 64 ? 1 : 2; }
+__host__ __device__ constexpr int pair_threads(int KT) { return 64 + 128 * pair_halves(KT); }
+constexpr int SCRATCH2 = 17;  // floats per epilogue thread (16-value slow-path passes)
 
 template <int KT>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(pair_threads(KT), 1)
     k_gemm_topk2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem =
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t *drain = acc_empty + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // 128 x 33 floats
+  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // epilogue threads x SCRATCH2 floats
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
@@ -401,7 +409,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&acc_full[a], 1);
-      mbar_init(&acc_empty[a], 8);  // 4 epilogue warps x 2 CTAs (leader's copy is used)
+      mbar_init(&acc_empty[a], 2 * 4 * pair_halves(KT));  // epilogue warps x 2 CTAs (leader's copy)
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -527,9 +535,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (both CTAs)
-    const int quarter = warp & 3;
+    constexpr int H = pair_halves(KT);
+    constexpr int CH = BN / 32 / H;        // 32-column chunks per warp and tile
+    const int quarter = warp & 3;          // TMEM lanes this warp may read
+    const int half = (warp - 2) >> 2;      // tile chunks [CH half, CH half + CH)
     const int row_in_tile = quarter * 32 + lane;
-    float *scratch = scratch_all + (threadIdx.x - 64) * 33;
+    float *scratch = scratch_all + (threadIdx.x - 64) * SCRATCH2;
     const bool f16 = g.score_mode == R2M_SCORE_F16;
     const bool scaled = g.score_mode == R2M_SCORE_SCALED;
     int acc = 0;
@@ -553,7 +564,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const long long colbase = (long long)t * BN;
         const bool tail = colbase + BN > g.N;
 #pragma unroll 1
-        for (int ch = 0; ch < BN / 32; ++ch) {
+        for (int ch = half * CH; ch < (half + 1) * CH; ++ch) {
           float v[32];
           __syncwarp();
           tmem_ld32(taddr + ch * 32, v);
@@ -586,12 +597,15 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (f16) mx = round_f16(mx);
           if (mx > R.thr) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) scratch[j] = v[j];
+            for (int p = 0; p < 2; ++p) {
+#pragma unroll
+              for (int j = 0; j < 16; ++j) scratch[j] = v[16 * p + j];
 #pragma unroll 1
-            for (int j = 0; j < 32; ++j) {
-              float x = scratch[j];
-              if (f16) x = round_f16(x);
-              if (x > R.thr) R.insert(x, (int)(c0 + j));
+              for (int j = 0; j < 16; ++j) {
+                float x = scratch[j];
+                if (f16) x = round_f16(x);
+                if (x > R.thr) R.insert(x, (int)(c0 + 16 * p + j));
+              }
             }
           }
         }
@@ -604,8 +618,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (!ok) break;
       const int row = mt * 256 + (int)rank * 128 + row_in_tile;
       if (row < g.nb) {
-        float *pv = g.part_vals + ((size_t)sp * g.mpad + row) * KT;
-        int *pc = g.part_cols + ((size_t)sp * g.mpad + row) * KT;
+        const size_t list = (size_t)sp * H + half;
+        float *pv = g.part_vals + (list * g.mpad + row) * KT;
+        int *pc = g.part_cols + (list * g.mpad + row) * KT;
 #pragma unroll
         for (int j = 0; j < KT; ++j) {
           pv[j] = R.v[j];
@@ -755,16 +770,16 @@ static size_t gemm_smem_bytes() {
 
 // Column splits for a given number of read tiles: enough units to keep
 // every CTA busy, chosen to minimise the last-wave imbalance.
-static int choose_splits(int m_tiles, int n_tiles, int ctas, int forced) {
+static int choose_splits(int m_tiles, int n_tiles, int ctas, int forced, int max_splits = MAX_SPLITS) {
   if (forced > 0) {
     int s = forced;
     if (s > n_tiles) s = n_tiles;
-    if (s > MAX_SPLITS) s = MAX_SPLITS;
+    if (s > max_splits) s = max_splits;
     return s < 1 ? 1 : s;
   }
   int smin = (4 * ctas + m_tiles - 1) / m_tiles;
   if (smin < 1) smin = 1;
-  int cap = n_tiles < MAX_SPLITS ? n_tiles : MAX_SPLITS;
+  int cap = n_tiles < max_splits ? n_tiles : max_splits;
   if (smin > cap) smin = cap;
   int best = smin;
   double best_eff = -1.0;
@@ -791,18 +806,19 @@ static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmA
   return R2M_OK;
 }
 
-static size_t gemm2_smem_bytes() {
-  return 1024 + (size_t)STAGES2 * 2 * HALF_TILE + (2 * STAGES2 + 5) * 8 + 16 + (size_t)BM * 33 * sizeof(float);
+static size_t gemm2_smem_bytes(int KT) {
+  return 1024 + (size_t)STAGES2 * 2 * HALF_TILE + (2 * STAGES2 + 5) * 8 + 16 +
+         (size_t)(pair_threads(KT) - 64) * SCRATCH2 * sizeof(float);
 }
 
 template <int KT>
 static int launch_gemm2(const CUtensorMap &mA, const CUtensorMap &mB, const GemmArgs &g, int pairs,
                         cudaStream_t st) {
-  size_t smem = gemm2_smem_bytes();
+  size_t smem = gemm2_smem_bytes(KT);
   R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk2<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(2 * pairs, 1, 1);
-  cfg.blockDim = dim3(THREADS, 1, 1);
+  cfg.blockDim = dim3(pair_threads(KT), 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -825,7 +841,7 @@ static int kernel_kind(int mode, int nb) {
 }
 
 // Split lists the workspace must hold for any batch height up to rows_cap.
-static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int mode) {
+static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int mode, int KT) {
   size_t lists = 0;
   for (int nb = BM; nb < rows_cap + BM; nb += BM) {
     int h = nb < rows_cap ? nb : rows_cap;
@@ -833,7 +849,8 @@ static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int 
     int tile = kind == 2 ? 256 : BM;
     int mt = (h + tile - 1) / tile;
     int c = kind == 2 ? (ctas / 2 > 0 ? ctas / 2 : 1) : ctas;
-    size_t l = (size_t)choose_splits(mt, n_tiles, c, forced) * mt * tile;
+    const int H = kind == 2 ? pair_halves(KT) : 1;  // partial lists per row and split
+    size_t l = (size_t)choose_splits(mt, n_tiles, c, forced, MAX_SPLITS / H) * H * mt * tile;
     if (l > lists) lists = l;
   }
   return lists;
@@ -917,7 +934,7 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
     return rc;
   }
   // workspace: the largest (read tiles x splits) any batch height can ask for
-  size_t lists = lists_needed(rows_cap, e->n_tiles, e->ctas, e->forced_splits, e->mode);
+  size_t lists = lists_needed(rows_cap, e->n_tiles, e->ctas, e->forced_splits, e->mode, e->KT);
   e->part_lists = lists;
   cudaError_t ce = cudaMalloc(&e->part_vals, lists * e->KT * sizeof(float));
   if (ce == cudaSuccess) ce = cudaMalloc(&e->part_cols, lists * e->KT * sizeof(int));
@@ -952,7 +969,7 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   const int ctas = tune->ctas > 0 ? tune->ctas : sm_count();
   const int forced = tune->splits > 0 ? tune->splits : 0;
   const int mode = (tune->reserved[1] >= 0 && tune->reserved[1] <= 2) ? tune->reserved[1] : 0;
-  size_t lists = lists_needed(eng->rows_cap, eng->n_tiles, ctas, forced, mode);
+  size_t lists = lists_needed(eng->rows_cap, eng->n_tiles, ctas, forced, mode, eng->KT);
   if (lists > eng->part_lists) {  // grow the split workspace
     float *pv = nullptr;
     int *pc = nullptr;
@@ -1025,7 +1042,9 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   g.num_m_tiles = (nb + tile - 1) / tile;
   g.N = eng->N;
   g.n_tiles = eng->n_tiles;
-  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits);
+  const int halves = kind == 2 ? pair_halves(eng->KT) : 1;  // partial lists per row and split
+  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / halves);
+  const int lists_per_row = halves * g.splits;
   g.num_kb = (eng->rdim + BK - 1) / BK;
   g.score_mode = eng->score_mode;
   g.mpad = g.num_m_tiles * tile;
@@ -1033,7 +1052,7 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   g.part_vals = eng->part_vals;
   g.part_cols = eng->part_cols;
   g.err = eng->err;
-  if ((size_t)g.splits * g.mpad > eng->part_lists) return fail(R2M_ESTATE, "engine workspace too small");
+  if ((size_t)lists_per_row * g.mpad > eng->part_lists) return fail(R2M_ESTATE, "engine workspace too small");
   long long units = (long long)g.num_m_tiles * g.splits;
   int ctas = (int)(units < ctas_eff ? units : ctas_eff);
   eng->last_splits = g.splits;
@@ -1059,7 +1078,7 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[1], st));
   const int warps = 8;
   k_merge_splits<<<(nb + warps - 1) / warps, 32 * warps, 0, st>>>(
-      eng->part_vals, eng->part_cols, g.splits, g.mpad, eng->KT, nb, eng->k, eng->score_mode, d_scaleA,
+      eng->part_vals, eng->part_cols, lists_per_row, g.mpad, eng->KT, nb, eng->k, eng->score_mode, d_scaleA,
       d_vals, d_locs);
   R2M_CUDA(cudaGetLastError());
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[2], st));
