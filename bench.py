@@ -422,7 +422,8 @@ def batching_leg(dev, n_requests: int, seed: int = 61):
            "index_cols": idx.N, "requests": n_requests, "reads": total,
            "ragged_graph_reads_per_s": total / t_ragged, "per_request_reads_per_s": total / t_each,
            "speedup": t_each / t_ragged, "first_run_s": t_first, "launch_sets": 1,
-           "autotuned": {"splits": s_best[0], "ctas": s_best[1], "candidates": tuner.log}}
+           "autotuned": {"splits": s_best[0], "ctas": s_best[1],
+                         "epilogue": s_best[2] if len(s_best) > 2 else "auto", "candidates": tuner.log}}
     eng.close()
     del idx, eng, b
     torch.cuda.empty_cache()

@@ -371,16 +371,21 @@ __global__ void __launch_bounds__(THREADS, 1)
 constexpr int STAGES2 = 6;
 constexpr int HALF_TILE = 128 * BK;  // 16 KiB
 // CTA-pair kernel: TMA warp, MMA warp and 4 * H epilogue warps.  With H = 2
-// (KT <= 32) two warps share each TMEM lane quarter, each draining one half
-// (128 columns) of every tile into its own reservoir, so a (read tile, column
-// split) unit leaves two partial lists per row; KT = 64 keeps one warp per
-// quarter (H = 1), whose larger reservoir needs the registers.
-__host__ __device__ constexpr int pair_halves(int KT) { return KT >= 64 ? 1 : 2; }
-__host__ __device__ constexpr int pair_threads(int KT) { return 64 + 128 * pair_halves(KT); }
+// two warps share each TMEM lane quarter, each draining one half (128
+// columns) of every tile into its own reservoir, so a (read tile, column
+// split) unit leaves two partial lists per row.  That halves the per-warp
+// latency chain of a tile and the reservoir warm-up at every unit start --
+// the gain of short units -- but keeps more warps busy, which under the
+// board's power cap lowers the clock of long units; the host picks H per
+// launch (pair_halves_for).  KT = 64 always uses H = 1 (its reservoir needs
+// the registers).
+__host__ __device__ constexpr int pair_threads(int H) { return 64 + 128 * H; }
 constexpr int SCRATCH2 = 17;  // floats per epilogue thread (16-value slow-path passes)
+// 256-column tiles per work unit at or below which the 8-warp epilogue pays
+constexpr int SHORT_UNIT_TILES = 8192;
 
-template <int KT>
-__global__ void __launch_bounds__(pair_threads(KT), 1)
+template <int KT, int H>
+__global__ void __launch_bounds__(pair_threads(H), 1)
     k_gemm_topk2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem =
@@ -409,7 +414,7 @@ __global__ void __launch_bounds__(pair_threads(KT), 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&acc_full[a], 1);
-      mbar_init(&acc_empty[a], 2 * 4 * pair_halves(KT));  // epilogue warps x 2 CTAs (leader's copy)
+      mbar_init(&acc_empty[a], 2 * 4 * H);  // epilogue warps x 2 CTAs (leader's copy is used)
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -535,7 +540,6 @@ __global__ void __launch_bounds__(pair_threads(KT), 1)
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (both CTAs)
-    constexpr int H = pair_halves(KT);
     constexpr int CH = BN / 32 / H;        // 32-column chunks per warp and tile
     const int quarter = warp & 3;          // TMEM lanes this warp may read
     const int half = (warp - 2) >> 2;      // tile chunks [CH half, CH half + CH)
@@ -806,19 +810,24 @@ static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmA
   return R2M_OK;
 }
 
-static size_t gemm2_smem_bytes(int KT) {
+static size_t gemm2_smem_bytes(int H) {
   return 1024 + (size_t)STAGES2 * 2 * HALF_TILE + (2 * STAGES2 + 5) * 8 + 16 +
-         (size_t)(pair_threads(KT) - 64) * SCRATCH2 * sizeof(float);
+         (size_t)(pair_threads(H) - 64) * SCRATCH2 * sizeof(float);
 }
 
-template <int KT>
+// Epilogue halves for a pair-kernel launch: 2 for short units (k <= 32).
+static int pair_halves_for(int KT, int n_tiles, int splits) {
+  return (KT <= 32 && (n_tiles + splits - 1) / splits <= SHORT_UNIT_TILES) ? 2 : 1;
+}
+
+template <int KT, int H>
 static int launch_gemm2(const CUtensorMap &mA, const CUtensorMap &mB, const GemmArgs &g, int pairs,
                         cudaStream_t st) {
-  size_t smem = gemm2_smem_bytes(KT);
-  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk2<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  size_t smem = gemm2_smem_bytes(H);
+  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk2<KT, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(2 * pairs, 1, 1);
-  cfg.blockDim = dim3(pair_threads(KT), 1, 1);
+  cfg.blockDim = dim3(pair_threads(H), 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -828,7 +837,7 @@ static int launch_gemm2(const CUtensorMap &mA, const CUtensorMap &mB, const Gemm
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  R2M_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_topk2<KT>, mA, mB, g));
+  R2M_CUDA(cudaLaunchKernelEx(&cfg, k_gemm_topk2<KT, H>, mA, mB, g));
   return R2M_OK;
 }
 
@@ -849,7 +858,8 @@ static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int 
     int tile = kind == 2 ? 256 : BM;
     int mt = (h + tile - 1) / tile;
     int c = kind == 2 ? (ctas / 2 > 0 ? ctas / 2 : 1) : ctas;
-    const int H = kind == 2 ? pair_halves(KT) : 1;  // partial lists per row and split
+    // the pair kernel may leave two partial lists per row and split
+    const int H = (kind == 2 && KT <= 32) ? 2 : 1;
     size_t l = (size_t)choose_splits(mt, n_tiles, c, forced, MAX_SPLITS / H) * H * mt * tile;
     if (l > lists) lists = l;
   }
@@ -875,6 +885,7 @@ struct r2m_engine {
   CUtensorMap mapB;
   CUtensorMap mapB128;  // 128-row box for the CTA-pair kernel
   int mode;             // 0 auto, 1 single-CTA kernel, 2 CTA-pair kernel
+  int epi;              // CTA-pair epilogue: 0 auto, 1 four warps, 2 eight warps
   float *part_vals;
   int *part_cols;
   size_t part_lists;  // capacity in lists (rows x splits)
@@ -916,6 +927,8 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   e->timing = tune && tune->reserved[0] != 0;
   e->mode = tune ? tune->reserved[1] : 0;
   if (e->mode < 0 || e->mode > 2) e->mode = 0;
+  e->epi = tune ? tune->reserved[2] : 0;
+  if (e->epi < 0 || e->epi > 2) e->epi = 0;
   e->last_splits = 0;
   if (e->timing) {
     for (int i = 0; i < 3; ++i) {
@@ -989,6 +1002,7 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   eng->ctas = ctas;
   eng->forced_splits = forced;
   eng->mode = mode;
+  eng->epi = (tune->reserved[2] >= 0 && tune->reserved[2] <= 2) ? tune->reserved[2] : 0;
   return R2M_OK;
 }
 
@@ -1042,9 +1056,12 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   g.num_m_tiles = (nb + tile - 1) / tile;
   g.N = eng->N;
   g.n_tiles = eng->n_tiles;
-  const int halves = kind == 2 ? pair_halves(eng->KT) : 1;  // partial lists per row and split
-  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / halves);
-  const int lists_per_row = halves * g.splits;
+  const int hmax = (kind == 2 && eng->KT <= 32) ? 2 : 1;
+  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / hmax);
+  int halves = 1;
+  if (kind == 2)
+    halves = eng->epi == 1 ? 1 : eng->epi == 2 ? hmax : pair_halves_for(eng->KT, eng->n_tiles, g.splits);
+  const int lists_per_row = halves * g.splits;  // partial lists each row leaves
   g.num_kb = (eng->rdim + BK - 1) / BK;
   g.score_mode = eng->score_mode;
   g.mpad = g.num_m_tiles * tile;
@@ -1058,12 +1075,21 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   eng->last_splits = g.splits;
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[0], st));
   if (kind == 2) {
-    switch (eng->KT) {
-      case 8: rc = launch_gemm2<8>(mapA, eng->mapB128, g, ctas, st); break;
-      case 16: rc = launch_gemm2<16>(mapA, eng->mapB128, g, ctas, st); break;
-      case 20: rc = launch_gemm2<20>(mapA, eng->mapB128, g, ctas, st); break;
-      case 32: rc = launch_gemm2<32>(mapA, eng->mapB128, g, ctas, st); break;
-      default: rc = launch_gemm2<64>(mapA, eng->mapB128, g, ctas, st); break;
+    if (halves == 2) {
+      switch (eng->KT) {
+        case 8: rc = launch_gemm2<8, 2>(mapA, eng->mapB128, g, ctas, st); break;
+        case 16: rc = launch_gemm2<16, 2>(mapA, eng->mapB128, g, ctas, st); break;
+        case 20: rc = launch_gemm2<20, 2>(mapA, eng->mapB128, g, ctas, st); break;
+        default: rc = launch_gemm2<32, 2>(mapA, eng->mapB128, g, ctas, st); break;
+      }
+    } else {
+      switch (eng->KT) {
+        case 8: rc = launch_gemm2<8, 1>(mapA, eng->mapB128, g, ctas, st); break;
+        case 16: rc = launch_gemm2<16, 1>(mapA, eng->mapB128, g, ctas, st); break;
+        case 20: rc = launch_gemm2<20, 1>(mapA, eng->mapB128, g, ctas, st); break;
+        case 32: rc = launch_gemm2<32, 1>(mapA, eng->mapB128, g, ctas, st); break;
+        default: rc = launch_gemm2<64, 1>(mapA, eng->mapB128, g, ctas, st); break;
+      }
     }
   } else {
     switch (eng->KT) {

@@ -33,7 +33,10 @@ def bucket_rows(n: int) -> int:
 
 
 class Autotuner:
-    """Picks (splits, ctas) for an engine and row count by timing candidates."""
+    """Picks (splits, ctas, epilogue) for an engine and row count by timing
+    candidates.  The CTA-pair epilogue form (4 or 8 warps) depends on how
+    long a work unit is, so it is only tuned when the candidates run on the
+    engine itself; on a proxy index the automatic rule stays."""
 
     def __init__(self, cache_path: str | None = None, reps: int = 2, proxy_cols: int = 0):
         self.reps = reps
@@ -67,8 +70,9 @@ class Autotuner:
     def tune(self, eng, A8: torch.Tensor, rows: int, scaleA=None, stream=None):
         k = self.key(eng, rows)
         if k in self.cache:
-            s, c = self.cache[k]
-            eng.set_tuning(s, c)
+            s, c, *rest = self.cache[k]
+            ep = rest[0] if rest else "auto"
+            eng.set_tuning(s, c, epilogue=ep)
             return s, c
         sms = torch.cuda.get_device_properties(eng.device).multi_processor_count
         st = stream or torch.cuda.current_stream(eng.device)
@@ -77,9 +81,8 @@ class Autotuner:
             from .engine import TopKEngine
             sb = eng.scaleB[:self.proxy_cols] if eng.scaleB is not None else None
             target = TopKEngine(eng.B[:self.proxy_cols], k=eng.k, rows_cap=eng.rows_cap, score=eng.score, scaleB=sb)
-        best, best_ms = (0, 0), float("inf")
-        for s, c in self.candidates(rows, eng.N, sms):
-            target.set_tuning(s, c)
+        def timed(s, c, ep):
+            target.set_tuning(s, c, epilogue=ep)
             target.search(A8, rows, scaleA, stream=st)  # warm
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
@@ -88,16 +91,26 @@ class Autotuner:
             e1.record(st)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / self.reps
-            self.log.append({"rows": rows, "splits": s, "ctas": c, "ms": ms})
+            self.log.append({"rows": rows, "splits": s, "ctas": c, "epilogue": ep, "ms": ms})
+            return ms
+
+        best, best_ms = (0, 0, "auto"), float("inf")
+        for s, c in self.candidates(rows, eng.N, sms):
+            ms = timed(s, c, "auto")
             if ms < best_ms:
-                best, best_ms = (s, c), ms
+                best, best_ms = (s, c, "auto"), ms
+        if target is eng and rows > 128 and eng.k <= 32:  # the CTA-pair kernel's epilogue forms
+            for ep in ("4", "8"):
+                ms = timed(best[0], best[1], ep)
+                if ms < best_ms:
+                    best, best_ms = (best[0], best[1], ep), ms
         if target is not eng:
             target.close()
-        eng.set_tuning(*best)
+        eng.set_tuning(best[0], best[1], epilogue=best[2])
         self.cache[k] = list(best)
         if self.path:
             self.path.write_text(json.dumps(self.cache))
-        return best
+        return best[0], best[1]
 
 
 class RaggedBatcher:

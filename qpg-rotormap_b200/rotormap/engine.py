@@ -18,6 +18,8 @@ from .encoder import RopeEncoder, encode_frag_real_batch, f16_to_f8
 from .fasta import DeviceFastaFragments, FastaFragments, fasta_reads, fasta_reads_device
 
 _MODES = {"f16": _lib.SCORE_F16, "f32": _lib.SCORE_F32, "scaled": _lib.SCORE_SCALED}
+# CTA-pair epilogue: auto, 4 warps, or 8 warps (two column halves; k <= 32)
+_EPILOGUES = {"auto": 0, "4": 1, "8": 2}
 # fused kernel variant: one CTA per 128-read tile, or CTA pairs (cta_group::2)
 # per 256-read tile; "auto" uses pairs above 128 reads
 _KERNELS = {"auto": 0, "1sm": 1, "2sm": 2}
@@ -53,7 +55,8 @@ class TopKEngine:
 
     def __init__(self, B: torch.Tensor, k: int = 20, w: int | None = None, rows_cap: int = 8192,
                  segs: int | None = None, score: str = "f16", scaleB: torch.Tensor | None = None,
-                 splits: int = 0, ctas: int = 0, timing: bool = False, kernel: str = "auto"):
+                 splits: int = 0, ctas: int = 0, timing: bool = False, kernel: str = "auto",
+                 epilogue: str = "auto"):
         _lib.require_device()
         if B.dtype != torch.uint8 or B.dim() != 2 or not B.is_cuda or not B.is_contiguous():
             raise ValueError("B must be a contiguous (N, rdim) uint8 CUDA tensor")
@@ -71,10 +74,13 @@ class TopKEngine:
         self.scaleA = torch.ones((rows_cap,), dtype=torch.float32, device=B.device)
         if kernel not in _KERNELS:
             raise ValueError("kernel must be 'auto', '1sm' or '2sm'")
+        if epilogue not in _EPILOGUES:
+            raise ValueError("epilogue must be 'auto', '4' or '8'")
         tune = Tuning(splits, ctas)
         tune.reserved[0] = 1 if timing else 0
         tune.reserved[1] = _KERNELS[kernel]
-        self.kernel = kernel
+        tune.reserved[2] = _EPILOGUES[epilogue]
+        self.kernel, self.epilogue = kernel, epilogue
         h = ctypes.c_void_p()
         check(lib().r2m_engine_create(ptr(B), ptr(scaleB), rdim, N, k, rows_cap, _MODES[score],
                                       ctypes.byref(tune), ctypes.byref(h)))
@@ -84,13 +90,18 @@ class TopKEngine:
     def device(self) -> torch.device:
         return self.B.device
 
-    def set_tuning(self, splits: int = 0, ctas: int = 0, kernel: str | None = None) -> None:
+    def set_tuning(self, splits: int = 0, ctas: int = 0, kernel: str | None = None,
+                   epilogue: str | None = None) -> None:
         """Change the schedule (0 = automatic).  Not during stream capture."""
         kernel = kernel or self.kernel
+        epilogue = epilogue or self.epilogue
+        if epilogue not in _EPILOGUES:
+            raise ValueError("epilogue must be 'auto', '4' or '8'")
         t = Tuning(splits, ctas)
         t.reserved[1] = _KERNELS[kernel]
+        t.reserved[2] = _EPILOGUES[epilogue]
         check(lib().r2m_engine_set_tuning(self._h, ctypes.byref(t)))
-        self.splits, self.ctas, self.kernel = splits, ctas, kernel
+        self.splits, self.ctas, self.kernel, self.epilogue = splits, ctas, kernel, epilogue
 
     def kernel_ms(self):
         """(gemm_ms, merge_ms, splits) of the last search (timing engines only)."""
