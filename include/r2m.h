@@ -236,6 +236,27 @@ int r2m_plain_batch_gemm_topk(r2m_plain_engine *eng, const uint8_t *d_A,
                               int nb, float *d_vals, int32_t *d_locs,
                               r2m_stream_t stream);
 
+/* ----------------------------------------------------------- match table */
+
+typedef struct r2m_text r2m_text;
+
+/* Replaces the table writer of run_map (RotorMap/tools/map.jl:141-151): one
+ * line per read and top-k hit, "<header without '>'> <+|-> <score> <window
+ * start - 1> <record name>\n", the score as Julia's string(::Float32).
+ * vals / locs: (nb, k) host arrays (locs 1-based column ids, 1..ncols);
+ * heads: nb headers, each followed by '\n'; strand / starts (1-based) /
+ * col_rec: per-column index tables; rec_names: the record names (first
+ * header token without '>'), each followed by '\n'.  nthreads host threads.
+ * Free the text with r2m_text_free. */
+int r2m_format_table(const float *vals, const int32_t *locs, int64_t nb, int k, const char *heads,
+                     size_t heads_len, const uint8_t *strand, const int64_t *starts, const int32_t *col_rec,
+                     int64_t ncols, const char *rec_names, size_t rec_names_len, int nthreads, r2m_text **out);
+const char *r2m_text_data(const r2m_text *t, size_t *len);
+void r2m_text_free(r2m_text *t);
+/* Julia's string(::Float32) of x into out (cap >= 32, NUL-terminated);
+ * returns its length, or a negative error code. */
+int r2m_format_f32(float x, char *out, size_t cap);
+
 /* ------------------------------------------------------- host-ring engine */
 
 typedef struct r2m_compact r2m_compact;

@@ -16,6 +16,9 @@ paths relative to the q4bio-qpg/qpg-rotormap tree):
   seg_topk_merge_ref  RotorMap/gemm/topk_kernels.jl:213-329 (segmented top-k,
                       its reservoir / merge tie rules)
   batch_topk_ref      RotorMap/search/engine_fp8.jl:399-437 (chunk loop)
+  julia_repr_f32_ref  Julia's string(::Float32), the score field of
+                      RotorMap/tools/map.jl:148
+  table_lines_ref     RotorMap/tools/map.jl:141-151 (match table lines)
 C restatements (oracle/rotormap_oracle.c, built by oracle/Makefile):
   rope_f64 / rope_f32 / f32_to_e4m3 / f32_to_f16 / topk_e4m3 / scores_e4m3.
 
@@ -29,6 +32,7 @@ vectors (tests/golden/), and the reference's committed experiment curves
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -419,3 +423,62 @@ def batch_topk_ref(scores: np.ndarray, w: int, K: int = 20, PS: int = 8):
     for lo in range(0, N, w):
         seg_topk_merge_ref(scores[:, lo:lo + w], lo, dv, dl, K, PS)
     return dv, dl
+
+
+# ---------------------------------------------------------------- match table
+
+
+def julia_repr_f32_ref(x: float) -> str:
+    """Julia's `string(::Float32)` (the score field of RotorMap/tools/map.jl:148):
+    shortest round-trip digits (numpy's float32 repr), decimal form when the
+    first significant digit's decimal exponent e has -5 < e < 6, else
+    `d.ddde±x`; NaN, Inf, -Inf, 0.0, -0.0 literal."""
+    x = np.float32(x)
+    if math.isnan(x):
+        return "NaN"
+    if math.isinf(x):
+        return "Inf" if x > 0 else "-Inf"
+    if x == 0:
+        return "-0.0" if math.copysign(1.0, float(x)) < 0 else "0.0"
+    r = repr(x)  # numpy: shortest round-trip for float32, e.g. '0.9873047' / '1e-05'
+    r = r.replace("np.float32(", "").rstrip(")")
+    sign = "-" if r.startswith("-") else ""
+    r = r.lstrip("-")
+    # split into digits and decimal exponent
+    if "e" in r:
+        mant, ex = r.split("e")
+        ex = int(ex)
+    else:
+        mant, ex = r, 0
+    if "." in mant:
+        ip, fp = mant.split(".")
+    else:
+        ip, fp = mant, ""
+    digits = (ip + fp).lstrip("0")
+    lead_zeros = len(ip + fp) - len((ip + fp).lstrip("0"))
+    # decimal exponent of the first significant digit
+    e10 = len(ip) - 1 + ex - lead_zeros
+    digits = digits.rstrip("0") or "0"
+    if -5 < e10 < 6:
+        if e10 >= 0:
+            ip2 = digits[:e10 + 1].ljust(e10 + 1, "0")
+            fp2 = digits[e10 + 1:] or "0"
+        else:
+            ip2 = "0"
+            fp2 = "0" * (-e10 - 1) + digits
+        return f"{sign}{ip2}.{fp2}"
+    fp2 = digits[1:] or "0"
+    return f"{sign}{digits[0]}.{fp2}e{e10}"
+
+
+def table_lines_ref(vals, locs, heads, strand, starts, col_rec, recname):
+    """The match lines of RotorMap/tools/map.jl:141-151 for one batch:
+    `<header without '>'> <+|-> <score> <starts[c]-1> <record name>`."""
+    lines = []
+    for r in range(vals.shape[0]):
+        hd = heads[r][1:] if heads[r].startswith(">") else heads[r]
+        for j in range(vals.shape[1]):
+            c = int(locs[r, j]) - 1
+            lines.append(f"{hd} {'+' if strand[c] == 0 else '-'} {julia_repr_f32_ref(vals[r, j])} "
+                         f"{int(starts[c]) - 1} {recname[col_rec[c]]}\n")
+    return "".join(lines)

@@ -67,6 +67,11 @@ SIGNATURES = [
     ("r2m_reads_header_blob", P, [P, ctypes.POINTER(SZ)]),
     ("r2m_reads_header_offsets", P, [P]),
     ("r2m_reads_free", None, [P]),
+    ("r2m_format_table", I, [P, P, I64, I, ctypes.c_char_p, SZ, P, P, P, I64, ctypes.c_char_p, SZ, I,
+                             ctypes.POINTER(P)]),
+    ("r2m_text_data", P, [P, ctypes.POINTER(SZ)]),
+    ("r2m_text_free", None, [P]),
+    ("r2m_format_f32", I, [ctypes.c_float, ctypes.c_char_p, SZ]),
     ("r2m_compact_create", I, [P, P, I, I64, I, I, I, I64, I, I, P, ctypes.POINTER(P)]),
     ("r2m_compact_destroy", I, [P]),
     ("r2m_compact_chunks", I64, [P]),

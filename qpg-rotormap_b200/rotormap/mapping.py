@@ -7,6 +7,7 @@ engine_fp8.jl:654-733 (map_and_count) and RotorMap/reads/provenance.jl:46-78
 from __future__ import annotations
 
 import math
+import os
 import time
 
 import numpy as np
@@ -60,61 +61,57 @@ def _no_gt(s: str) -> str:
     return s[1:] if s.startswith(">") else s
 
 
-def julia_repr_f32(x: float) -> str:
-    """Julia's `string(::Float32)`: shortest round-trip digits, decimal form
-    for 1e-4 <= |x| < 1e6, else `d.ddde±x` (the score field of map.jl:148)."""
-    x = np.float32(x)
-    if math.isnan(x):
-        return "NaN"
-    if math.isinf(x):
-        return "Inf" if x > 0 else "-Inf"
-    if x == 0:
-        return "-0.0" if math.copysign(1.0, float(x)) < 0 else "0.0"
-    r = repr(x)  # numpy: shortest round-trip for float32, e.g. '0.9873047' / '1e-05'
-    r = r.replace("np.float32(", "").rstrip(")")
-    sign = "-" if r.startswith("-") else ""
-    r = r.lstrip("-")
-    # split into digits and decimal exponent
-    if "e" in r:
-        mant, ex = r.split("e")
-        ex = int(ex)
-    else:
-        mant, ex = r, 0
-    if "." in mant:
-        ip, fp = mant.split(".")
-    else:
-        ip, fp = mant, ""
-    digits = (ip + fp).lstrip("0")
-    lead_zeros = len(ip + fp) - len((ip + fp).lstrip("0"))
-    # decimal exponent of the first significant digit
-    e10 = len(ip) - 1 + ex - lead_zeros
-    digits = digits.rstrip("0") or "0"
-    if -5 < e10 < 6:
-        if e10 >= 0:
-            ip2 = digits[:e10 + 1].ljust(e10 + 1, "0")
-            fp2 = digits[e10 + 1:] or "0"
-        else:
-            ip2 = "0"
-            fp2 = "0" * (-e10 - 1) + digits
-        return f"{sign}{ip2}.{fp2}"
-    fp2 = digits[1:] or "0"
-    return f"{sign}{digits[0]}.{fp2}e{e10}"
-
-
-def write_table(io, vals, locs, heads, idx: Index, recname=None) -> int:
+def write_table(io, vals, locs, heads, idx: Index, recname=None, nthreads: int | None = None) -> int:
     """Write map.jl's match lines for one batch (map.jl:141-151):
-    `<read hdr sans '>'> <+|-> <score> <starts[c]-1> <record first token>`."""
+    `<read hdr sans '>'> <+|-> <score> <starts[c]-1> <record first token>`,
+    formatted by the library's native writer (r2m_format_table).  `io` may be
+    a binary or a text stream."""
+    import ctypes
+    import io as _io
+
+    from ._lib import check, lib
     if recname is None:
         recname = [_no_gt(h.split()[0]) if h.split() else "" for h in idx.rec_heads]
-    lines = []
-    for r in range(vals.shape[0]):
-        hd = _no_gt(heads[r])
-        for j in range(vals.shape[1]):
-            c = int(locs[r, j]) - 1
-            lines.append(f"{hd} {'+' if idx.strand[c] == 0 else '-'} {julia_repr_f32(vals[r, j])} "
-                         f"{int(idx.starts[c]) - 1} {recname[idx.col_rec[c]]}\n")
-    io.write("".join(lines))
-    return len(lines)
+    vals = np.ascontiguousarray(vals, np.float32)
+    locs = np.ascontiguousarray(locs, np.int32)
+    nb, k = vals.shape
+    if nb == 0:
+        return 0
+    hb = ("\n".join(heads) + "\n").encode("latin-1")
+    rb = ("\n".join(recname) + "\n").encode("latin-1")
+    strand = np.ascontiguousarray(idx.strand, np.uint8)
+    starts = np.ascontiguousarray(idx.starts, np.int64)
+    col_rec = np.ascontiguousarray(idx.col_rec, np.int32)
+    L = lib()
+    h = ctypes.c_void_p()
+    check(L.r2m_format_table(vals.ctypes.data, locs.ctypes.data, nb, k, hb, len(hb), strand.ctypes.data,
+                             starts.ctypes.data, col_rec.ctypes.data, strand.size, rb, len(rb),
+                             nthreads or (os.cpu_count() or 1), ctypes.byref(h)))
+    try:
+        n = ctypes.c_size_t()
+        p = L.r2m_text_data(h, ctypes.byref(n))
+        data = ctypes.string_at(p, n.value)
+    finally:
+        L.r2m_text_free(h)
+    if isinstance(io, _io.TextIOBase):
+        io.write(data.decode("latin-1"))
+    else:
+        io.write(data)
+    return nb * k
+
+
+def julia_repr_f32(x: float) -> str:
+    """Julia's `string(::Float32)` (the score field of map.jl:148): shortest
+    round-trip digits, decimal form for 1e-4 <= |x| < 1e6, else `d.ddde±x`;
+    formatted by the library (r2m_format_f32)."""
+    import ctypes
+
+    from ._lib import lib
+    buf = ctypes.create_string_buffer(48)
+    n = lib().r2m_format_f32(float(x), buf, 48)
+    if n < 0:
+        raise ValueError("format failed")
+    return buf.value.decode()
 
 
 def run_map(index, reads, out=None, topk: int = 20, batch_size: int = 8192, verbose: bool = False,
@@ -132,7 +129,7 @@ def run_map(index, reads, out=None, topk: int = 20, batch_size: int = 8192, verb
     score = score or ("scaled" if idx.scaled else "f16")
     recname = [_no_gt(h.split()[0]) if h.split() else "" for h in idx.rec_heads]
     n = 0
-    with open(out, "w") as io:
+    with open(out, "wb") as io:
         for bat in rope_topk_stream(idx.encoder, reads, B, k=topk, batch_size=batch_size, score=score,
                                     scaleB=sb):
             write_table(io, bat.vals, bat.locs, bat.heads, idx, recname)

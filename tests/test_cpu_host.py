@@ -286,3 +286,48 @@ def test_mutate_edits_follows_the_reference_model():
     a = synth.mutate_edits(codes, 0.2, np.random.default_rng(11))
     b = synth.mutate_edits(codes, 0.2, np.random.default_rng(11))
     assert np.array_equal(a, b)
+
+
+def test_native_float_format_matches_oracle_on_random_bits():
+    """r2m_format_f32 (the table's score field) against the oracle's
+    restatement of Julia's string(::Float32) on random float32 bit patterns
+    spanning every exponent, plus subnormals, extremes and the literals."""
+    rng = np.random.default_rng(5)
+    bits = rng.integers(0, 2 ** 32, 20_000, dtype=np.uint64).astype(np.uint32)
+    xs = bits.view(np.float32)
+    extra = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 1e-45, -1e-45, 1.1754944e-38, 3.4028235e38,
+                      1e-4, 9.999999e-5, 1e6, 999999.94, 0.1, 0.3, 2.5, 100.0, 1e-5, 123456.0], np.float32)
+    for x in np.concatenate([xs, extra]):
+        assert rm.julia_repr_f32(x) == orc.julia_repr_f32_ref(x), (float(x), x.view(np.uint32))
+
+
+@pytest.mark.parametrize("nb", [1, 37, 5000])
+def test_native_table_matches_oracle(nb, tmp_path):
+    """write_table (r2m_format_table, threaded above 2048 reads) writes the
+    oracle's map.jl lines byte for byte, to text and to binary streams."""
+    import io as _io
+    from rotormap.mapping import write_table
+
+    class Idx:
+        pass
+    rng = np.random.default_rng(nb)
+    N, k = 50_000, 20
+    idx = Idx()
+    idx.strand = rng.integers(0, 2, N).astype(np.uint8)
+    idx.starts = rng.integers(1, 10 ** 9, N).astype(np.int64)
+    idx.col_rec = rng.integers(0, 3, N).astype(np.int32)
+    idx.rec_heads = [">chr1 one", ">chrX", ">scaffold_7 len=5"]
+    vals = (rng.standard_normal((nb, k)) * 10.0 ** rng.integers(-7, 8, (nb, k))).astype(np.float32)
+    locs = rng.integers(1, N + 1, (nb, k)).astype(np.int32)
+    heads = [f">read_{i} start={i} len=150 src=chr1" if i % 3 else f"noangle_{i}" for i in range(nb)]
+    want = orc.table_lines_ref(vals, locs, heads, idx.strand, idx.starts, idx.col_rec, ["chr1", "chrX", "scaffold_7"])
+    t = _io.StringIO()
+    assert write_table(t, vals, locs, heads, idx) == nb * k
+    assert t.getvalue() == want
+    b = _io.BytesIO()
+    write_table(b, vals, locs, heads, idx, nthreads=3)
+    assert b.getvalue().decode() == want
+    bad = locs.copy()
+    bad[0, 0] = N + 1
+    with pytest.raises(rm.R2MError):
+        write_table(_io.BytesIO(), vals, bad, heads, idx)
