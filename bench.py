@@ -491,6 +491,62 @@ def compact_leg(dev, ncols: int = 4_194_304, chunk: int = 1 << 20, seed: int = 8
     return out
 
 
+def map_leg(dev, n_reads: int = 400_000, ncols: int = 1_048_576, seed: int = 91):
+    """run_map end to end (RotorMap/tools/map.jl): a FASTA file of n_reads
+    150 bp reads (5% substitutions, provenance headers) sampled from a seeded
+    genome, mapped against its index of `ncols` columns (k = 150, stride 15,
+    f16 scores, top-20) and written as the match table -- FASTA parse (GPU or
+    host reader), encode, fused search and the threaded table writer
+    overlapped with the next batch.  Compared with the search alone."""
+    import tempfile
+
+    import torch
+
+    import rotormap as rm
+    from rotormap import synth
+    re = rm.RopeEncoder(k=K_BASES, s=S, m=M, c=C)
+    nbases = (ncols // 2 - 1) * KSTEP + K_BASES
+    words, woff, nb, runs = synth.random_genome_packed([nbases], seed=seed, gc=0.41, device=dev)
+    idx = rm.build_index_packed(re, words, [">chr1 synthetic"], woff, nb, KSTEP)
+    recs, offs = synth.sample_positions(nb, runs, n_reads, K_BASES, seed)
+    rw = synth.extract_reads_packed(words, woff, recs, offs, K_BASES, 0.05, seed)
+    del words
+    j = np.arange(K_BASES)
+    codes = ((rw[:, j >> 4] >> (2 * (j & 15)).astype(np.uint32)) & 3).astype(np.uint8)
+    letters = synth.LETTERS[codes]
+    raw = b"".join(b">read_%d start=%d len=150 src=chr1\n" % (i + 1, offs[i] + 1) + letters[i].tobytes() + b"\n"
+                   for i in range(n_reads))
+    out = {"workload": f"{n_reads} reads x 150 bp FASTA ({len(raw)} bytes) vs {idx.N} columns, f16 top-20, "
+                       f"batches of 65,536; table of {n_reads * TOPK} lines"}
+    with tempfile.TemporaryDirectory() as tdir:
+        fa = os.path.join(tdir, "reads.fa")
+        with open(fa, "wb") as f:
+            f.write(raw)
+        rm.run_map(idx, fa, os.path.join(tdir, "warm.maps"), topk=TOPK, batch_size=65_536)
+        for reader in ("device", "host"):
+            dst = os.path.join(tdir, f"{reader}.maps")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            n = rm.run_map(idx, fa, dst, topk=TOPK, batch_size=65_536, reader=reader)
+            dt = time.perf_counter() - t0
+            with open(dst, "rb") as f:
+                lines = sum(1 for _ in f)
+            out[f"run_map_{reader}_reader"] = {"seconds": dt, "reads_per_s": n / dt, "lines": lines}
+    eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=65_536)
+    a8, _ = rm.encode_frag_real_batch_alloc(torch.uint8, re, torch.from_numpy(rw[:65_536].view(np.int32)).to(dev))
+    eng.search(a8)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        eng.search(a8)
+    torch.cuda.synchronize()
+    out["search_only_reads_per_s"] = 3 * 65_536 / (time.perf_counter() - t0)
+    eng.close()
+    del idx, eng, a8
+    torch.cuda.empty_cache()
+    return out
+
+
 def fasta_leg(dev, n_reads: int = 400_000, seed: int = 71):
     """Reads-side FASTA parsing: the native host reader (all cores) against
     the GPU reader, on a FASTA of n_reads 150 bp reads with provenance-style
@@ -565,6 +621,7 @@ def main():
     ap.add_argument("--no-batching", action="store_true", help="skip the batching leg")
     ap.add_argument("--no-fasta", action="store_true", help="skip the FASTA reader leg")
     ap.add_argument("--no-compact", action="store_true", help="skip the host-ring engine leg")
+    ap.add_argument("--no-map", action="store_true", help="skip the run_map end-to-end leg")
     ap.add_argument("--batching-requests", type=int, default=48)
     ap.add_argument("--precision-reads", type=int, default=100_000)
     ap.add_argument("--precision-sample", type=int, default=1000)
@@ -715,6 +772,8 @@ def main():
             line["fasta_reader"] = fasta_leg(dev)
         if world == 1 and not args.no_compact:
             line["compact"] = compact_leg(dev)
+        if world == 1 and not args.no_map:
+            line["run_map"] = map_leg(dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -115,9 +115,15 @@ def julia_repr_f32(x: float) -> str:
 
 
 def run_map(index, reads, out=None, topk: int = 20, batch_size: int = 8192, verbose: bool = False,
-            score: str | None = None) -> int:
+            score: str | None = None, reader: str = "device") -> int:
     """run_map (map.jl:100-184): INDEX + READS -> the match table at `out`
-    (default READS + ".maps").  Returns the number of reads mapped."""
+    (default READS + ".maps").  Returns the number of reads mapped.
+
+    The table of batch i is formatted and written by a writer thread (the
+    native formatter releases the GIL) while the GPU maps batch i+1."""
+    import queue
+    import threading
+
     idx = index if isinstance(index, Index) else load_index(index)
     out = out or (str(reads) + ".maps")
     t0 = time.perf_counter()
@@ -129,11 +135,35 @@ def run_map(index, reads, out=None, topk: int = 20, batch_size: int = 8192, verb
     score = score or ("scaled" if idx.scaled else "f16")
     recname = [_no_gt(h.split()[0]) if h.split() else "" for h in idx.rec_heads]
     n = 0
+    q: queue.Queue = queue.Queue(maxsize=2)
+    failure: list = []
+
+    def writer(io):
+        while True:
+            bat = q.get()
+            if bat is None:
+                return
+            if not failure:
+                try:
+                    write_table(io, bat.vals, bat.locs, bat.heads, idx, recname)
+                except BaseException as e:  # reported by the caller after the join
+                    failure.append(e)
+
     with open(out, "wb") as io:
-        for bat in rope_topk_stream(idx.encoder, reads, B, k=topk, batch_size=batch_size, score=score,
-                                    scaleB=sb):
-            write_table(io, bat.vals, bat.locs, bat.heads, idx, recname)
-            n += len(bat.heads)
+        th = threading.Thread(target=writer, args=(io,), daemon=True)
+        th.start()
+        try:
+            for bat in rope_topk_stream(idx.encoder, reads, B, k=topk, batch_size=batch_size, score=score,
+                                        scaleB=sb, reader=reader):
+                if failure:
+                    break
+                q.put(bat)
+                n += len(bat.heads)
+        finally:
+            q.put(None)
+            th.join()
+    if failure:
+        raise failure[0]
     if verbose:
         t = time.perf_counter() - t0
         print(f"MAPPED {n} reads -> {out} ({n * topk} match lines) in {t:.2f} s")
