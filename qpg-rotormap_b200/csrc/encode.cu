@@ -40,7 +40,7 @@ struct EncParams {
   uint32_t bmask, cbmask, csmerG;
   float theta[8];  // per idm, fp32
   int table_in_smem;
-  int hist_floats;  // per-warp histogram floats (2*nbin, rounded to 4)
+  int hist_floats;  // per-warp histogram floats (2*nbin, rounded to whole 16-bin chunks)
   int cs_u16;       // per-warp csmer slots (nw rounded up to 8)
   int words_u32;    // per-warp staged words (W + 2, rounded up to 4)
 };
@@ -71,7 +71,7 @@ static int make_params(EncParams &P, int k, int s, int m, int c, int normalize) 
     float f = (m == 1) ? 1.0f : (float)(2.0 * (double)i / (double)(m - 1) + 1.0);
     P.theta[i] = f * base;
   }
-  P.hist_floats = (P.rdim + 3) & ~3;
+  P.hist_floats = (P.rdim + 31) & ~31;
   P.cs_u16 = (P.nw + 7) & ~7;
   P.words_u32 = (P.W + 2 + 3) & ~3;
   return R2M_OK;
@@ -183,6 +183,17 @@ __device__ __forceinline__ void store1(void *row, int i, float v) {
   }
 }
 
+// Shared-memory histogram layout.  Complex bin cb (Re, Im adjacent) lives in
+// chunk j = cb / 16 (32 floats = 8 float4 slots), complex slot w = cb % 16,
+// float4 slot w / 2 -- stored at slot (w / 2) ^ (j % 8).  The output passes
+// give each lane one chunk and walk its 8 slots in order; without the XOR
+// every lane of a step would hit the same four banks (chunks are 128 bytes
+// apart), with it the 32 lanes of a step cover all 32 banks.
+__device__ __forceinline__ int hoff(int cb) {
+  const int j = cb >> 4, w = cb & 15;
+  return ((((j << 3) | ((w >> 1) ^ (j & 7))) << 2) | ((w & 1) << 1));
+}
+
 // Value of output element i (split layout) before the storage conversion.
 // E4M3 parity mode rounds through fp16 first, like the reference's fp16
 // stream followed by f32_to_f8 of the widened value.
@@ -192,7 +203,7 @@ __device__ __forceinline__ float out_value(const EncParams &P, const float *hist
   int bin = (i < P.nbin) ? i : i - P.nbin;
   int part = (i < P.nbin) ? 0 : 1;
   float nrm = nrmv[P.normalize == 0 ? 0 : (bin % P.m)];
-  float x = hist[2 * bin + part] / nrm;
+  float x = hist[hoff(bin) + part] / nrm;
   if constexpr (OUT == R2M_OUT_E4M3) x = __half2float(__float2half_rn(x));
   if constexpr (OUT == R2M_OUT_E4M3_SCALED) x = x * scale;
   return x;
@@ -234,17 +245,21 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
       if (lane == __ffs(grp) - 1) {
         if (P.m == 4 && grp == (1u << lane)) {
           // common case: a window alone in its bin within the batch
-          float4 *h = reinterpret_cast<float4 *>(hist + 2 * (cbin * 4));
-          float4 h01 = h[0], h23 = h[1];
+          // bins 4 cbin .. 4 cbin + 3: float4 slots 2 (cbin % 4) and the next
+          // one of chunk cbin / 4, swizzled
+          float4 *hc = reinterpret_cast<float4 *>(hist + ((cbin >> 2) << 5));
+          const int sw = (int)((cbin >> 2) & 7), s0 = (int)(2 * (cbin & 3));
+          float4 *h0 = hc + (s0 ^ sw), *h1 = hc + ((s0 + 1) ^ sw);
+          float4 h01 = *h0, h23 = *h1;
           const float2 p0 = table[b0 + lane], p1 = table[(size_t)P.nw + b0 + lane];
           const float2 p2 = table[2 * (size_t)P.nw + b0 + lane], p3 = table[3 * (size_t)P.nw + b0 + lane];
           h01.x += p0.x; h01.y += p0.y; h01.z += p1.x; h01.w += p1.y;
           h23.x += p2.x; h23.y += p2.y; h23.z += p3.x; h23.w += p3.y;
-          h[0] = h01;
-          h[1] = h23;
+          *h0 = h01;
+          *h1 = h23;
         } else {
           for (int idm = 0; idm < P.m; ++idm) {
-            float *h = hist + 2 * (cbin * P.m + idm);
+            float *h = hist + hoff((int)(cbin * P.m + idm));
             float re = h[0], im = h[1];
             const float2 *tb = table + (size_t)idm * P.nw + b0;
             unsigned g = grp;
@@ -265,7 +280,7 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
   }
   // zero the G-homopolymer bins
   if (lane < P.m) {
-    float *h = hist + 2 * (P.csmerG * P.m + lane);
+    float *h = hist + hoff(P.csmerG * P.m + lane);
     h[0] = 0.f;
     h[1] = 0.f;
   }
@@ -273,11 +288,12 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
   // modes 2/3 reshape every bin first (fp64 arithmetic, fp32 storage)
   if (P.normalize >= 2) {
     for (int b = lane; b < P.nbin; b += 32) {
-      float re = hist[2 * b], im = hist[2 * b + 1];
+      float *h = hist + hoff(b);
+      float re = h[0], im = h[1];
       double a = (double)hypotf(re, im);
       double d = (P.normalize == 2) ? (a + 2.220446049250313e-16) : sqrt(a + 2.220446049250313e-16);
-      hist[2 * b] = (float)((double)re / d);
-      hist[2 * b + 1] = (float)((double)im / d);
+      h[0] = (float)((double)re / d);
+      h[1] = (float)((double)im / d);
     }
     __syncwarp();
   }
@@ -290,9 +306,8 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
     // accumulator, then a butterfly over the lanes of the same copy (the
     // lanes of other copies would only add zeros, so the sums are the same)
     float acc = 0.f;
-    const float2 *h2 = reinterpret_cast<const float2 *>(hist);
     for (int b = lane; b < P.nbin; b += 32) {
-      float2 z = h2[b];
+      float2 z = *reinterpret_cast<const float2 *>(hist + hoff(b));
       acc += __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
     }
     for (int o = 16; o >= P.m; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
@@ -300,7 +315,8 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
     for (int q = 0; q < 8; ++q) part[q] = __shfl_sync(FULL, acc, q < P.m ? q : 0);
   } else {
     for (int b = lane; b < P.nbin; b += 32) {
-      float re = hist[2 * b], im = hist[2 * b + 1];
+      const float *h = hist + hoff(b);
+      float re = h[0], im = h[1];
       float e = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
       int t = b % P.m;
 #pragma unroll
@@ -361,16 +377,17 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
     float amax = 0.f;
     for (int j = lane; j < nchunk; j += 32) {
       float4 *h4 = reinterpret_cast<float4 *>(hist + 32 * j);
+      const int sw = j & 7;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        float4 t = h4[q];
+        float4 t = h4[q ^ sw];
         t.x = divn(t.x);
         t.y = divn(t.y);
         t.z = divn(t.z);
         t.w = divn(t.w);
         if constexpr (OUT == R2M_OUT_E4M3_SCALED)
           amax = fmaxf(amax, fmaxf(fmaxf(fabsf(t.x), fabsf(t.y)), fmaxf(fabsf(t.z), fabsf(t.w))));
-        h4[q] = t;
+        h4[q ^ sw] = t;
       }
     }
     float scale = 1.0f;
@@ -382,10 +399,11 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
     }
     for (int j = lane; j < nchunk; j += 32) {
       const float4 *h4 = reinterpret_cast<const float4 *>(hist + 32 * j);
+      const int sw = j & 7;
       float re[16], im[16];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        float4 t = h4[q];
+        float4 t = h4[q ^ sw];
         re[2 * q] = t.x;
         im[2 * q] = t.y;
         re[2 * q + 1] = t.z;
