@@ -215,7 +215,7 @@ __device__ __forceinline__ float out_value(const EncParams &P, const float *hist
 // of every copy (index 0 for mode 0) and `norms_out` the reference's norms
 // row.  The normalised value of split element i is hist[...]/nrmv[...].
 __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *table, float *hist, uint16_t *cs,
-                              const uint32_t *words, float *nrmv, float *norms_out) {
+                              const uint32_t *words, float *nrmv, float *norms_out, float *amax_raw = nullptr) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
   // zero the histogram
@@ -305,23 +305,36 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
     // every bin of this lane (b = lane + 32j) belongs to copy lane % m: one
     // accumulator, then a butterfly over the lanes of the same copy (the
     // lanes of other copies would only add zeros, so the sums are the same)
-    float acc = 0.f;
+    float acc = 0.f, mx = 0.f;
     for (int b = lane; b < P.nbin; b += 32) {
       float2 z = *reinterpret_cast<const float2 *>(hist + hoff(b));
       acc += __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
+      mx = fmaxf(mx, fmaxf(fabsf(z.x), fabsf(z.y)));
+    }
+    if (amax_raw) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+      *amax_raw = mx;
     }
     for (int o = 16; o >= P.m; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
 #pragma unroll
     for (int q = 0; q < 8; ++q) part[q] = __shfl_sync(FULL, acc, q < P.m ? q : 0);
   } else {
+    float mx = 0.f;
     for (int b = lane; b < P.nbin; b += 32) {
       const float *h = hist + hoff(b);
       float re = h[0], im = h[1];
       float e = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
+      mx = fmaxf(mx, fmaxf(fabsf(re), fabsf(im)));
       int t = b % P.m;
 #pragma unroll
       for (int q = 0; q < 8; ++q)
         if (q == t) part[q] += e;
+    }
+    if (amax_raw) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+      *amax_raw = mx;
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -359,10 +372,12 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
                                 float *norms_out, float *scale_out) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
-  fragment_hist(P, table, hist, cs, words, nrmv, norms_out);
-  if (P.normalize == 0 && (P.nbin % 16) == 0 && P.nbin >= 16) {
-    // 16 bins per lane chunk: divide in place (one division per value), then
-    // convert and store the chunk's Re and Im runs (16 values each)
+  const bool fast = P.normalize == 0 && (P.nbin % 16) == 0 && P.nbin >= 16;
+  float amax_raw = 0.f;
+  fragment_hist(P, table, hist, cs, words, nrmv, norms_out, fast ? &amax_raw : nullptr);
+  if (fast) {
+    // one output pass: each lane takes chunks of 16 bins, divides every value
+    // by the norm, scales, converts and stores the chunk's Re and Im runs
     const float nrm = nrmv[0];
     // x / nrm for every value with one reciprocal: y = RN(1/nrm), q0 = x*y,
     // r = x - q0*nrm (exact with FMA), q = RN(q0 + r*y) is the correctly
@@ -374,26 +389,11 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
       return fmaf(r, y, q0);
     };
     const int nchunk = P.nbin >> 4;
-    float amax = 0.f;
-    for (int j = lane; j < nchunk; j += 32) {
-      float4 *h4 = reinterpret_cast<float4 *>(hist + 32 * j);
-      const int sw = j & 7;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        float4 t = h4[q ^ sw];
-        t.x = divn(t.x);
-        t.y = divn(t.y);
-        t.z = divn(t.z);
-        t.w = divn(t.w);
-        if constexpr (OUT == R2M_OUT_E4M3_SCALED)
-          amax = fmaxf(amax, fmaxf(fmaxf(fabsf(t.x), fabsf(t.y)), fmaxf(fabsf(t.z), fabsf(t.w))));
-        h4[q ^ sw] = t;
-      }
-    }
     float scale = 1.0f;
     if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(FULL, amax, o));
+      // a correctly rounded division is monotone and odd, so the largest
+      // normalised magnitude is the largest raw magnitude divided once
+      const float amax = divn(amax_raw);
       scale = amax > 0.f ? 448.0f / amax : 1.0f;
       if (lane == 0) *scale_out = amax > 0.f ? amax / 448.0f : 0.0f;
     }
@@ -404,10 +404,10 @@ __device__ void encode_fragment(const EncParams &P, const float2 *table, float *
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         float4 t = h4[q ^ sw];
-        re[2 * q] = t.x;
-        im[2 * q] = t.y;
-        re[2 * q + 1] = t.z;
-        im[2 * q + 1] = t.w;
+        re[2 * q] = divn(t.x);
+        im[2 * q] = divn(t.y);
+        re[2 * q + 1] = divn(t.z);
+        im[2 * q + 1] = divn(t.w);
       }
       if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
 #pragma unroll
