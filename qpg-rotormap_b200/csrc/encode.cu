@@ -243,18 +243,23 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
       uint32_t cbin = cs[p];
       unsigned grp = __match_any_sync(amask, cbin);
       if (lane == __ffs(grp) - 1) {
-        if (P.m == 4 && grp == (1u << lane)) {
-          // common case: a window alone in its bin within the batch
-          // bins 4 cbin .. 4 cbin + 3: float4 slots 2 (cbin % 4) and the next
-          // one of chunk cbin / 4, swizzled
+        if (P.m == 4) {
+          // the group's bins 4 cbin .. 4 cbin + 3 (float4 slots 2 (cbin % 4)
+          // and the next one of chunk cbin / 4, swizzled): one read-modify-
+          // write, the members' phasors added in window (lane) order
           float4 *hc = reinterpret_cast<float4 *>(hist + ((cbin >> 2) << 5));
           const int sw = (int)((cbin >> 2) & 7), s0 = (int)(2 * (cbin & 3));
           float4 *h0 = hc + (s0 ^ sw), *h1 = hc + ((s0 + 1) ^ sw);
           float4 h01 = *h0, h23 = *h1;
-          const float2 p0 = table[b0 + lane], p1 = table[(size_t)P.nw + b0 + lane];
-          const float2 p2 = table[2 * (size_t)P.nw + b0 + lane], p3 = table[3 * (size_t)P.nw + b0 + lane];
-          h01.x += p0.x; h01.y += p0.y; h01.z += p1.x; h01.w += p1.y;
-          h23.x += p2.x; h23.y += p2.y; h23.z += p3.x; h23.w += p3.y;
+          unsigned g = grp;
+          do {
+            const int j = __ffs(g) - 1;
+            g &= g - 1;
+            const float2 p0 = table[b0 + j], p1 = table[(size_t)P.nw + b0 + j];
+            const float2 p2 = table[2 * (size_t)P.nw + b0 + j], p3 = table[3 * (size_t)P.nw + b0 + j];
+            h01.x += p0.x; h01.y += p0.y; h01.z += p1.x; h01.w += p1.y;
+            h23.x += p2.x; h23.y += p2.y; h23.z += p3.x; h23.w += p3.y;
+          } while (g);
           *h0 = h01;
           *h1 = h23;
         } else {
@@ -301,7 +306,45 @@ __device__ __forceinline__ void fragment_hist(const EncParams &P, const float2 *
   float part[8];
 #pragma unroll
   for (int t = 0; t < 8; ++t) part[t] = 0.f;
-  if ((32 % P.m) == 0) {
+  if (P.m <= 4 && (P.hist_floats & 127) == 0) {
+    // walk the histogram linearly in float4 slots (the order of a sum of
+    // squares is free): slot s of chunk j holds complex bins 2w', 2w' + 1 of
+    // the chunk, w' = s ^ (j % 8), i.e. copies 2(w' & 1) and 2(w' & 1) + 1
+    // for m = 4, copies 0 and 1 for m = 2, copy 0 for m = 1
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, mx = 0.f;
+    const float4 *h4 = reinterpret_cast<const float4 *>(hist);
+    const int nslot = P.hist_floats >> 2;
+    for (int i = lane; i < nslot; i += 32) {
+      const float4 t = h4[i];
+      const float e0 = __fadd_rn(__fmul_rn(t.x, t.x), __fmul_rn(t.y, t.y));
+      const float e1 = __fadd_rn(__fmul_rn(t.z, t.z), __fmul_rn(t.w, t.w));
+      mx = fmaxf(mx, fmaxf(fmaxf(fabsf(t.x), fabsf(t.y)), fmaxf(fabsf(t.z), fabsf(t.w))));
+      const bool hi = (((i & 7) ^ ((i >> 3) & 7)) & 1) != 0;  // w' odd: copies 2, 3
+      if (hi) {
+        a2 += e0;
+        a3 += e1;
+      } else {
+        a0 += e0;
+        a1 += e1;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(FULL, a0, o);
+      a1 += __shfl_xor_sync(FULL, a1, o);
+      a2 += __shfl_xor_sync(FULL, a2, o);
+      a3 += __shfl_xor_sync(FULL, a3, o);
+      mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+    }
+    if (P.m == 4) {
+      part[0] = a0, part[1] = a1, part[2] = a2, part[3] = a3;
+    } else if (P.m == 2) {
+      part[0] = a0 + a2, part[1] = a1 + a3;
+    } else {
+      part[0] = (a0 + a2) + (a1 + a3);
+    }
+    if (amax_raw) *amax_raw = mx;
+  } else if ((32 % P.m) == 0) {
     // every bin of this lane (b = lane + 32j) belongs to copy lane % m: one
     // accumulator, then a butterfly over the lanes of the same copy (the
     // lanes of other copies would only add zeros, so the sums are the same)
