@@ -166,17 +166,41 @@ extern "C" int r2m_fasta_reads(const char *data, size_t len, int k, int nthreads
       th.emplace_back(parse_range, data, len, cuts[i], cuts[i + 1], k, std::ref(parts[i]));
     for (auto &t : th) t.join();
   }
-  for (size_t i = 0; i < np; ++i) {
-    Part &p = parts[i];
-    r->words.insert(r->words.end(), p.words.begin(), p.words.end());
-    size_t off = 0;
+  // the parse ends at the first part that met an unclosed header (that part
+  // keeps the records before it); place every kept part at its offset
+  size_t keep = 0;
+  while (keep < np && !parts[keep].stop) ++keep;
+  if (keep < np) ++keep;
+  std::vector<size_t> wofs(keep + 1, 0), hofs(keep + 1, 0), rofs(keep + 1, 0);
+  for (size_t i = 0; i < keep; ++i) {
+    wofs[i + 1] = wofs[i] + parts[i].words.size();
+    hofs[i + 1] = hofs[i] + parts[i].heads.size() + parts[i].hlen.size();  // + one '\n' per header
+    rofs[i + 1] = rofs[i] + parts[i].hlen.size();
+  }
+  r->words.resize(wofs[keep]);
+  r->heads.resize(hofs[keep]);
+  r->hoff.resize(rofs[keep] + 1);
+  r->hoff[0] = 0;
+  auto place = [&](size_t i) {
+    const Part &p = parts[i];
+    if (!p.words.empty()) memcpy(r->words.data() + wofs[i], p.words.data(), p.words.size() * sizeof(uint32_t));
+    char *dst = &r->heads[0] + hofs[i];
+    size_t src = 0, o = hofs[i];
     for (size_t j = 0; j < p.hlen.size(); ++j) {
-      r->heads.append(p.heads, off, p.hlen[j]);
-      r->heads.push_back('\n');
-      off += p.hlen[j];
-      r->hoff.push_back(r->heads.size());
+      memcpy(dst, p.heads.data() + src, p.hlen[j]);
+      dst += p.hlen[j];
+      *dst++ = '\n';
+      src += p.hlen[j];
+      o += p.hlen[j] + 1;
+      r->hoff[rofs[i] + j + 1] = o;
     }
-    if (p.stop) break;  // parse ends at an unterminated header line
+  };
+  if (keep <= 1) {
+    if (keep) place(0);
+  } else {
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < keep; ++i) th.emplace_back(place, i);
+    for (auto &t : th) t.join();
   }
   *out = r;
   return R2M_OK;

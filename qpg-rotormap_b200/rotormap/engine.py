@@ -7,6 +7,7 @@ double-buffered C chunks have no counterpart: scores never leave TMEM.
 from __future__ import annotations
 
 import ctypes
+from collections.abc import Sequence
 from dataclasses import dataclass
 
 import numpy as np
@@ -29,11 +30,12 @@ _KERNELS = {"auto": 0, "1sm": 1, "2sm": 2}
 class TopKBatch:
     """One batch of results (engine_fp8.jl:265-271): vals (nb, k) float32
     descending, locs (nb, k) int32 1-based global column ids, norms (nb, m),
-    heads, first (1-based global index of the batch's first read)."""
+    heads (a sequence of strings), first (1-based global index of the batch's
+    first read)."""
     vals: np.ndarray
     locs: np.ndarray
     norms: np.ndarray
-    heads: list
+    heads: Sequence
     first: int
 
 
@@ -398,7 +400,7 @@ def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stre
             locs = D_loc.to("cpu", non_blocking=True)
             nrm = norms.to("cpu", non_blocking=True)
         st.synchronize()
-        yield TopKBatch(vals.numpy(), locs.numpy(), nrm.numpy(), list(heads), first0 + 1)
+        yield TopKBatch(vals.numpy(), locs.numpy(), nrm.numpy(), heads, first0 + 1)
 
 
 def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int | None = None,

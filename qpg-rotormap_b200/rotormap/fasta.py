@@ -10,6 +10,7 @@ from __future__ import annotations
 import ctypes
 import mmap
 import os
+from collections.abc import Sequence
 from dataclasses import dataclass
 
 import numpy as np
@@ -17,12 +18,66 @@ import numpy as np
 from ._lib import check, lib, ptr, require_device, stream_handle
 
 
+class HeaderList(Sequence):
+    """Read headers kept as one blob (every header followed by '\n'; headers
+    hold no '\n') with their start offsets: an item is decoded when it is
+    read, a slice is a view of the same blob, and the list compares equal to
+    a list of the same strings.  The table writer takes the blob as is."""
+
+    __slots__ = ("_blob", "_off")
+
+    def __init__(self, blob: bytes, offsets):
+        self._blob = blob
+        self._off = np.asarray(offsets, np.int64)  # n + 1 offsets; header i ends at off[i + 1] - 1
+
+    @classmethod
+    def from_blob(cls, blob: bytes) -> "HeaderList":
+        ends = np.flatnonzero(np.frombuffer(blob, np.uint8) == 0x0A)
+        return cls(blob, np.concatenate([[0], ends + 1]))
+
+    def __len__(self) -> int:
+        return self._off.size - 1
+
+    def __getitem__(self, i):
+        n = len(self)
+        if isinstance(i, slice):
+            start, stop, step = i.indices(n)
+            if step != 1:
+                return [self[j] for j in range(start, stop, step)]
+            stop = max(stop, start)
+            return HeaderList(self._blob, self._off[start:stop + 1])
+        if i < 0:
+            i += n
+        if not 0 <= i < n:
+            raise IndexError("header index out of range")
+        return self._blob[self._off[i]:self._off[i + 1] - 1].decode("latin-1")
+
+    def __iter__(self):
+        if len(self) == 0:
+            return iter(())
+        return iter(self.blob().decode("latin-1").split("\n")[:-1])
+
+    def blob(self) -> bytes:
+        """The headers of this list, each followed by '\n'."""
+        if len(self) == 0:
+            return b""
+        return self._blob[self._off[0]:self._off[-1]]
+
+    def __eq__(self, other):
+        if isinstance(other, (list, tuple, HeaderList)):
+            return list(self) == list(other)
+        return NotImplemented
+
+    def __repr__(self) -> str:
+        return f"HeaderList({len(self)} headers)"
+
+
 @dataclass
 class FastaFragments:
     """All kept records: words (n, cld(k,16)) uint32, verbatim '>' headers."""
     k: int
     words: np.ndarray
-    heads: list
+    heads: Sequence
 
     def __len__(self) -> int:
         return len(self.heads)
@@ -68,12 +123,13 @@ def fasta_reads(src, k: int = 20_000, parts: int | None = None) -> FastaFragment
             words = words.reshape(cnt, W)
         else:
             words = np.zeros((0, W), np.uint32)
-        heads = []
+        heads = HeaderList(b"", [0])
         if cnt:
             tot = ctypes.c_size_t()
             bp = L.r2m_reads_header_blob(handle, ctypes.byref(tot))
-            # every header is followed by one '\n' and contains none
-            heads = ctypes.string_at(bp, tot.value).decode("latin-1").split("\n")[:cnt]
+            op = L.r2m_reads_header_offsets(handle)
+            offs = np.ctypeslib.as_array((ctypes.c_size_t * (cnt + 1)).from_address(op)).astype(np.int64)
+            heads = HeaderList(ctypes.string_at(bp, tot.value), offs)
     finally:
         L.r2m_reads_free(handle)
         if keep is not None:
@@ -88,7 +144,7 @@ class DeviceFastaFragments:
     device (the uint32 bit pattern), verbatim '>' headers on the host."""
     k: int
     words: "torch.Tensor"
-    heads: list
+    heads: Sequence
 
     def __len__(self) -> int:
         return len(self.heads)
@@ -127,17 +183,28 @@ def fasta_reads_device(src, k: int = 20_000, device=None, stream=None) -> Device
         dev = dev_bytes.device
         host = None
     else:
-        data = _read_bytes(src)
-        host = np.frombuffer(data, np.uint8) if len(data) else np.zeros(0, np.uint8)
+        host = None
+        if not isinstance(src, (bytes, bytearray, memoryview)):
+            path = os.fspath(src)
+            size = os.path.getsize(path)
+        else:
+            host = np.frombuffer(src, np.uint8) if len(src) else np.zeros(0, np.uint8)
+            size = host.size
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         dev_bytes = None
     st = stream if stream is not None else torch.cuda.current_stream(dev)
     L = lib()
     with torch.cuda.device(dev), torch.cuda.stream(st):
         if dev_bytes is None:
-            stage = _pinned("fasta_in", host.size)
-            if host.size:
-                stage.numpy()[:] = host
+            stage = _pinned("fasta_in", size)
+            if size:
+                if host is not None:
+                    stage.numpy()[:] = host
+                else:  # read the file straight into the pinned buffer
+                    with open(path, "rb") as f:
+                        got = f.readinto(memoryview(stage.numpy()))
+                    if got != size:
+                        raise OSError(f"short read of {path}: {got} of {size} bytes")
             dev_bytes = stage.to(dev, non_blocking=True)
         handle = ctypes.c_void_p()
         n = int(dev_bytes.numel())
@@ -146,7 +213,7 @@ def fasta_reads_device(src, k: int = 20_000, device=None, stream=None) -> Device
             cnt = int(L.r2m_dreads_count(handle))
             W = (k + 15) // 16
             words = torch.empty((cnt, W), dtype=torch.int32, device=dev)
-            heads = []
+            heads = HeaderList(b"", [0])
             if cnt:
                 words.view(-1).copy_(_wrap_device(L.r2m_dreads_words(handle), cnt * W, torch.int32, dev))
                 tot = ctypes.c_size_t()
@@ -154,7 +221,7 @@ def fasta_reads_device(src, k: int = 20_000, device=None, stream=None) -> Device
                 hb = _pinned("fasta_heads", tot.value)
                 hb.copy_(_wrap_device(hp, tot.value, torch.uint8, dev), non_blocking=True)
                 st.synchronize()
-                heads = hb.numpy().tobytes().decode("latin-1").split("\n")[:cnt]
+                heads = HeaderList.from_blob(hb.numpy().tobytes())
         finally:
             st.synchronize()
             L.r2m_dreads_free(handle)

@@ -77,7 +77,11 @@ def write_table(io, vals, locs, heads, idx: Index, recname=None, nthreads: int |
     nb, k = vals.shape
     if nb == 0:
         return 0
-    hb = ("\n".join(heads) + "\n").encode("latin-1")
+    from .fasta import HeaderList
+    if isinstance(heads, HeaderList):
+        hb = heads.blob()
+    else:
+        hb = ("\n".join(heads) + "\n").encode("latin-1")
     rb = ("\n".join(recname) + "\n").encode("latin-1")
     strand = np.ascontiguousarray(idx.strand, np.uint8)
     starts = np.ascontiguousarray(idx.starts, np.int64)

@@ -331,3 +331,17 @@ def test_native_table_matches_oracle(nb, tmp_path):
     bad[0, 0] = N + 1
     with pytest.raises(rm.R2MError):
         write_table(_io.BytesIO(), vals, bad, heads, idx)
+
+
+def test_header_list_behaves_like_a_list():
+    hs = [">a one", ">b", "", ">c three words", ">" + "x" * 300]
+    blob = ("\n".join(hs) + "\n").encode()
+    hl = rm.HeaderList.from_blob(blob)
+    assert len(hl) == 5 and list(hl) == hs and hl == hs and hs == hl
+    assert hl[0] == ">a one" and hl[-1] == hs[-1] and hl[2] == ""
+    assert hl[1:4] == hs[1:4] and len(hl[1:4]) == 3 and hl[1:4].blob() == ("\n".join(hs[1:4]) + "\n").encode()
+    assert hl[::2] == hs[::2] and hl[3:1] == [] and list(hl[5:]) == []
+    with pytest.raises(IndexError):
+        hl[5]
+    f = rm.fasta_reads(b">r1 x\nACGT\n>r2\nAAAA\n", k=4)
+    assert isinstance(f.heads, rm.HeaderList) and f.heads == [">r1 x", ">r2"]
