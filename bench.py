@@ -491,6 +491,48 @@ def compact_leg(dev, ncols: int = 4_194_304, chunk: int = 1 << 20, seed: int = 8
     return out
 
 
+def gemm_bar_leg(dev, seconds: float = 2.0):
+    """The GEMM bar of the reference's production engine: cuBLASLt's fp8
+    GEMM (through torch._scaled_mm, which calls it) at the engine's chunk
+    shape -- M = 8,192 reads, K = 2,048, N = 65,536 index columns, e4m3
+    operands, fp32 accumulation, fp16 C (RotorMap/gemm/fp8_lt.jl:95-168) --
+    without any top-k.  Timed as a burst (20 calls) and as a loop of about
+    `seconds` (the power-capped regime the fused kernel's ~1.8 s launches
+    run in).  A measurement of the library, not part of this path."""
+    import torch
+    M, K, N = 8192, 2048, 65536
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    a = (torch.rand((M, K), generator=g, device=dev) * 2 - 1).to(torch.float8_e4m3fn)
+    b = (torch.rand((N, K), generator=g, device=dev) * 2 - 1).to(torch.float8_e4m3fn)
+    one = torch.ones((), dtype=torch.float32, device=dev)
+
+    def run():
+        return torch._scaled_mm(a, b.t(), scale_a=one, scale_b=one, out_dtype=torch.float16)
+
+    for _ in range(3):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(20):
+        run()
+    e1.record()
+    e1.synchronize()
+    burst_ms = e0.elapsed_time(e1) / 20
+    reps = max(20, int(seconds * 1e3 / max(burst_ms, 1e-3)))
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    e1.synchronize()
+    sus_ms = e0.elapsed_time(e1) / reps
+    flop = 2.0 * M * K * N
+    return {"library": "cuBLASLt fp8 via torch._scaled_mm", "shape": {"M": M, "K": K, "N": N},
+            "out": "fp16", "burst_ms": burst_ms, "burst_tflops": flop / burst_ms / 1e9,
+            "sustained_ms": sus_ms, "sustained_tflops": flop / sus_ms / 1e9, "sustained_calls": reps}
+
+
 def map_leg(dev, n_reads: int = 400_000, ncols: int = 1_048_576, seed: int = 91):
     """run_map end to end (RotorMap/tools/map.jl): a FASTA file of n_reads
     150 bp reads (5% substitutions, provenance headers) sampled from a seeded
@@ -622,6 +664,7 @@ def main():
     ap.add_argument("--no-fasta", action="store_true", help="skip the FASTA reader leg")
     ap.add_argument("--no-compact", action="store_true", help="skip the host-ring engine leg")
     ap.add_argument("--no-map", action="store_true", help="skip the run_map end-to-end leg")
+    ap.add_argument("--no-gemm-bar", action="store_true", help="skip the cuBLASLt fp8 GEMM bar")
     ap.add_argument("--batching-requests", type=int, default=48)
     ap.add_argument("--precision-reads", type=int, default=100_000)
     ap.add_argument("--precision-sample", type=int, default=1000)
@@ -774,6 +817,8 @@ def main():
             line["compact"] = compact_leg(dev)
         if world == 1 and not args.no_map:
             line["run_map"] = map_leg(dev)
+        if world == 1 and not args.no_gemm_bar:
+            line["gemm_bar"] = gemm_bar_leg(dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
