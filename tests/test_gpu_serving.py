@@ -1,8 +1,8 @@
 """Serving form: continuous batching over the resident index.
 
-Each request's result must be the same alone and in the mix (the north-star
-serving contract), requests must be admitted within the HBM budget, and the
-served results must agree with the plain batch path."""
+Each request's result must be the same alone and in the mix (the serving
+contract), requests must be admitted within the HBM budget, and the served
+results must agree with the plain batch path."""
 import threading
 import time
 
