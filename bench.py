@@ -478,15 +478,22 @@ def compact_leg(dev, ncols: int = 4_194_304, chunk: int = 1 << 20, seed: int = 8
         e1.synchronize()
         return e0.elapsed_time(e1) / 3, v, l
 
+    # the same host index with half of it kept on the device (2 of 4 chunks)
+    half = rm.CompactEngine(Bh, k=TOPK, rows_cap=65_536, score="scaled", scaleB=sb, chunk_cols=chunk, depth=3,
+                            pin=True, resident_chunks=2)
     for nq in (65_536, 8_192):
         ms_r, v0, l0 = timed(res, nq)
         ms_c, v1, l1 = timed(ring, nq)
+        ms_h, v2, l2 = timed(half, nq)
         out[f"q{nq}"] = {"resident_reads_per_s": nq / ms_r * 1e3, "ring_reads_per_s": nq / ms_c * 1e3,
                          "ring_over_resident": ms_r / ms_c, "ring_h2d_GBps": Bh.nbytes / ms_c / 1e6,
-                         "identical": bool(torch.equal(v0, v1) and torch.equal(l0, l1))}
+                         "half_resident_reads_per_s": nq / ms_h * 1e3, "half_resident_over_resident": ms_r / ms_h,
+                         "identical": bool(torch.equal(v0, v1) and torch.equal(l0, l1)
+                                           and torch.equal(v0, v2) and torch.equal(l0, l2))}
+    half.close()
     ring.close()
     res.close()
-    del idx, res, ring, Bh, a8, sa, dw, sb
+    del idx, res, ring, half, Bh, a8, sa, dw, sb
     torch.cuda.empty_cache()
     return out
 

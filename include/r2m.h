@@ -264,15 +264,19 @@ typedef struct r2m_compact r2m_compact;
 /* Replaces CompactEngine (RotorMap/search/engine_compact.jl:256-289): the
  * index h_B (N, rdim) e4m3 stays in HOST memory and is streamed through a
  * ring of `depth` device slots of about chunk_cols columns on its own H2D
- * stream.  d_scaleB (scaled scores) is a device vector of N column scales.
- * pin != 0 page-locks h_B for the engine's lifetime (read-only
- * registration; left pageable when the system refuses).  The host memory
- * must stay valid and unchanged while the engine lives. */
+ * stream.  The first resident_chunks chunks instead get device slots of
+ * their own, filled once (an index somewhat larger than the device keeps
+ * most of itself resident and streams only the rest).  d_scaleB (scaled
+ * scores) is a device vector of N column scales.  pin != 0 page-locks h_B
+ * for the engine's lifetime (read-only registration; left pageable when the
+ * system refuses).  The host memory must stay valid and unchanged while the
+ * engine lives. */
 int r2m_compact_create(const uint8_t *h_B, const float *d_scaleB, int rdim, int64_t N, int k, int rows_cap,
-                       int score_mode, int64_t chunk_cols, int depth, int pin, const r2m_tuning *tune,
-                       r2m_compact **out);
+                       int score_mode, int64_t chunk_cols, int depth, int resident_chunks, int pin,
+                       const r2m_tuning *tune, r2m_compact **out);
 int r2m_compact_destroy(r2m_compact *c);
 int64_t r2m_compact_chunks(const r2m_compact *c);
+int64_t r2m_compact_resident_chunks(const r2m_compact *c);
 int r2m_compact_is_pinned(const r2m_compact *c);
 /* Replaces batch_gemm_topk_compact! (RotorMap/search/engine_compact.jl:
  * 300-343): the same results as r2m_batch_gemm_topk over the whole index

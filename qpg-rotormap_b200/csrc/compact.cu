@@ -20,8 +20,12 @@
 // multiplies by scaleA last): chunk searches run with a unit row scale and
 // one final pass multiplies by scaleA with the same single rounding.
 //
-// When every chunk has its own slot (chunks <= depth) a chunk is copied once
-// and stays, so a small host index becomes resident after the first search.
+// The first `resident` chunks get slots of their own: each is copied once
+// and stays (an index a little larger than the device keeps most of itself in
+// HBM and streams only the rest); the remaining chunks go through the ring
+// of `depth` slots -- or also get slots of their own when they are no more
+// than `depth`.  A search visits the chunks in column order, so the resident
+// ones are searched while the first streamed ones are in flight.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -38,7 +42,7 @@ using namespace r2m;
 struct r2m_compact {
   const uint8_t *hB = nullptr;
   const float *d_scaleB = nullptr;
-  int rdim = 0, k = 0, rows_cap = 0, score_mode = 0, depth = 0;
+  int rdim = 0, k = 0, rows_cap = 0, score_mode = 0, depth = 0, resident = 0;
   int64_t N = 0, cap = 0;
   std::vector<int64_t> lo, wi;  // chunk column ranges
   std::vector<uint8_t *> slot;
@@ -122,8 +126,8 @@ void destroy(r2m_compact *c) {
 }  // namespace
 
 extern "C" int r2m_compact_create(const uint8_t *h_B, const float *d_scaleB, int rdim, int64_t N, int k,
-                                  int rows_cap, int score_mode, int64_t chunk_cols, int depth, int pin,
-                                  const r2m_tuning *tune, r2m_compact **out) {
+                                  int rows_cap, int score_mode, int64_t chunk_cols, int depth,
+                                  int resident_chunks, int pin, const r2m_tuning *tune, r2m_compact **out) {
   R2M_REQUIRE(out != nullptr, "out is null");
   *out = nullptr;
   R2M_REQUIRE(h_B != nullptr, "host B is null");
@@ -133,6 +137,7 @@ extern "C" int r2m_compact_create(const uint8_t *h_B, const float *d_scaleB, int
   R2M_REQUIRE(rows_cap >= 1, "rows_cap must be >= 1");
   R2M_REQUIRE(depth >= 2, "ring depth must be >= 2");
   R2M_REQUIRE(chunk_cols >= 256, "chunk_cols must be >= 256");
+  R2M_REQUIRE(resident_chunks >= 0, "resident_chunks must be >= 0");
   R2M_REQUIRE(score_mode >= R2M_SCORE_F16 && score_mode <= R2M_SCORE_SCALED, "bad score_mode");
   R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || d_scaleB, "scaled scores need scaleB (device)");
   R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || (reinterpret_cast<uintptr_t>(d_scaleB) & 15) == 0,
@@ -158,7 +163,9 @@ extern "C" int r2m_compact_create(const uint8_t *h_B, const float *d_scaleB, int
     c->cap = std::max(c->cap, c->wi.back());
   }
   cudaError_t e;
-  const int nslots = (int)std::min<int64_t>(depth, nch);
+  c->resident = (int)std::min<int64_t>(resident_chunks, nch);
+  const int64_t rest = nch - c->resident;
+  const int nslots = c->resident + (int)std::min<int64_t>(depth, rest);
   for (int b = 0; b < nslots; ++b) {
     uint8_t *p = nullptr;
     if ((e = cudaMalloc(&p, (size_t)c->cap * rdim)) != cudaSuccess) {
@@ -229,6 +236,8 @@ extern "C" int64_t r2m_compact_chunks(const r2m_compact *c) { return c ? (int64_
 
 extern "C" int r2m_compact_is_pinned(const r2m_compact *c) { return c && c->registered ? 1 : 0; }
 
+extern "C" int64_t r2m_compact_resident_chunks(const r2m_compact *c) { return c ? c->resident : 0; }
+
 extern "C" int r2m_compact_batch_gemm_topk(r2m_compact *c, const uint8_t *d_A, const float *d_scaleA, int nb,
                                            float *d_vals, int32_t *d_locs, r2m_stream_t stream) {
   R2M_REQUIRE(c != nullptr, "engine is null");
@@ -239,10 +248,12 @@ extern "C" int r2m_compact_batch_gemm_topk(r2m_compact *c, const uint8_t *d_A, c
   R2M_REQUIRE(!scaled || d_scaleA, "scaled scores need scaleA");
   cudaStream_t st = as_stream(stream);
   const int64_t nch = (int64_t)c->lo.size();
-  const int nslots = (int)c->slot.size();
-  const bool fixed = nch <= nslots;  // every chunk has its own slot
+  const int R = c->resident;
+  const int nring = (int)c->slot.size() - R;
+  const bool all_fixed = nch - R <= nring;  // the streamed chunks fit their own slots too
   for (int64_t i = 0; i < nch; ++i) {
-    const int b = fixed ? (int)i : (int)(c->next++ % nslots);
+    const bool fixed = i < R || all_fixed;
+    const int b = fixed ? (int)i : R + (int)(c->next++ % nring);
     if (c->holds[b] != i) {
       if (c->used[b]) R2M_CUDA(cudaStreamWaitEvent(c->h2d, c->ev_dev[b], 0));
       R2M_CUDA(cudaMemcpyAsync(c->slot[b], c->hB + (size_t)c->lo[i] * c->rdim, (size_t)c->wi[i] * c->rdim,

@@ -203,13 +203,17 @@ class CompactEngine:
     (a memory-mapped index file works) or a CPU uint8 tensor -- and each
     search streams it through `depth` device slots of about `chunk_cols`
     columns.  Same search() contract and the same results, bit for bit, as
-    TopKEngine over the whole index.  pin page-locks the host index for the
-    engine's lifetime (full-speed DMA; refused registrations stay pageable).
-    scaleB (scaled scores) is uploaded once (4 bytes per column)."""
+    TopKEngine over the whole index.  resident_chunks leading chunks get
+    device slots of their own, copied once ("auto": as many as the free
+    device memory holds beside the ring and a 2 GiB reserve), so only the
+    rest crosses the host link on every search.  pin page-locks the host
+    index for the engine's lifetime (full-speed DMA; refused registrations
+    stay pageable).  scaleB (scaled scores) is uploaded once (4 bytes per
+    column)."""
 
     def __init__(self, Bh, k: int = 20, rows_cap: int = 8192, score: str = "f16", scaleB=None,
                  chunk_cols: int = 1 << 20, depth: int = 3, pin: bool = True, device=None, splits: int = 0,
-                 ctas: int = 0, kernel: str = "auto"):
+                 ctas: int = 0, kernel: str = "auto", resident_chunks=0):
         _lib.require_device()
         if isinstance(Bh, torch.Tensor):
             if Bh.is_cuda or Bh.dtype != torch.uint8 or Bh.dim() != 2:
@@ -241,11 +245,30 @@ class CompactEngine:
         self.scaleA = torch.ones((rows_cap,), dtype=torch.float32, device=self._device)
         tune = Tuning(splits, ctas)
         tune.reserved[1] = _KERNELS[kernel]
+        if resident_chunks == "auto":
+            resident_chunks = self.auto_resident_chunks(self.N, rdim, chunk_cols, depth, self._device)
+        if int(resident_chunks) < 0:
+            raise ValueError("resident_chunks must be >= 0 or 'auto'")
         h = ctypes.c_void_p()
         with torch.cuda.device(self._device):
             check(lib().r2m_compact_create(addr, ptr(self.scaleB), self.rdim, self.N, k, rows_cap, _MODES[score],
-                                           chunk_cols, depth, 1 if pin else 0, ctypes.byref(tune), ctypes.byref(h)))
+                                           chunk_cols, depth, int(resident_chunks), 1 if pin else 0,
+                                           ctypes.byref(tune), ctypes.byref(h)))
         self._h = h
+
+    @staticmethod
+    def auto_resident_chunks(N: int, rdim: int, chunk_cols: int, depth: int, device=None,
+                             reserve: int = 2 << 30) -> int:
+        """Chunks that fit in the device memory free now beside the ring's
+        `depth` slots and `reserve` bytes."""
+        nch = -(-N // chunk_cols)
+        slot = (-(-N // nch) + 4) * rdim
+        free, _ = torch.cuda.mem_get_info(device)
+        return int(max(0, min(nch, (free - reserve - depth * slot) // slot)))
+
+    @property
+    def resident_chunks(self) -> int:
+        return int(lib().r2m_compact_resident_chunks(self._h))
 
     @property
     def device(self) -> torch.device:
@@ -443,13 +466,14 @@ def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size:
                              rows_cap: int | None = None, normalize: int = 0, score: str = "f16",
                              scaleB=None, resident: bool | None = None, chunk_cols: int = 1 << 20,
                              depth: int = 3, pin: bool = True, reader: str = "device", parts: int | None = None,
-                             stream=None):
+                             stream=None, resident_chunks="auto"):
     """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index
     Bh (N, rdim) uint8.  resident = None applies resident_fits: an index that
     fits beside the engine's working set is uploaded once and searched by
     the resident engine; otherwise (or resident = False) it stays in host
-    memory and every batch streams it through the CompactEngine ring.  Both
-    give the same batches."""
+    memory and the CompactEngine keeps resident_chunks of it on the device
+    ("auto": as many as fit) and streams the rest through its ring for every
+    batch.  Both give the same batches."""
     Bh = np.asarray(Bh) if not isinstance(Bh, torch.Tensor) else Bh
     nbytes = Bh.nbytes if isinstance(Bh, np.ndarray) else Bh.numel()
     cap = rows_cap or batch_size
@@ -470,7 +494,7 @@ def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size:
     if Bh.shape[1] != re.rdim:
         raise ValueError(f"B is {tuple(Bh.shape)}; the encoder's real embedding dim is {re.rdim}")
     eng = CompactEngine(Bh, k=k, rows_cap=cap, score=score, scaleB=sb, chunk_cols=chunk_cols, depth=depth,
-                        pin=pin)
+                        pin=pin, resident_chunks=resident_chunks)
     try:
         if reader == "device":
             frags = fasta_reads_device(file, k=re.k, device=eng.device, stream=stream)

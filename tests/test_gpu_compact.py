@@ -119,3 +119,33 @@ def test_compact_stream_ring_equals_resident(tmp_path):
     assert [x.heads for x in a] == [x.heads for x in b]
     for x, y in zip(a, b):
         assert np.array_equal(x.vals, y.vals) and np.array_equal(x.locs, y.locs)
+
+
+@pytest.mark.parametrize("nres,depth", [(1, 2), (2, 2), (3, 3), (5, 2), (9, 2), (0, 2)])
+@pytest.mark.parametrize("score", ["f16", "scaled"])
+def test_ring_with_resident_chunks(nres, depth, score):
+    """Leading chunks kept on the device (copied once), the rest streamed
+    through the ring (or given slots of their own when they are few): the
+    same results as the resident engine, search after search."""
+    rng = np.random.default_rng(nres * 7 + depth)
+    nb, N, rdim = 160, 30_000, 128
+    A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
+    B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
+    sa = rng.uniform(0.5, 2.0, nb).astype(np.float32) if score == "scaled" else None
+    sb = rng.uniform(0.5, 2.0, N).astype(np.float32) if score == "scaled" else None
+    v0, l0 = resident(A8, B8, 20, score, sa, sb)
+    eng = rm.CompactEngine(B8, k=20, rows_cap=nb, score=score, scaleB=sb, chunk_cols=6000, depth=depth,
+                           resident_chunks=nres)
+    assert eng.chunks == 5 and eng.resident_chunks == min(nres, 5)
+    A = torch.from_numpy(A8).cuda()
+    sat = torch.from_numpy(sa).cuda() if sa is not None else None
+    for _ in range(3):
+        v, l = eng.search(A, nb, sat)
+        assert np.array_equal(v.cpu().numpy(), v0) and np.array_equal(l.cpu().numpy(), l0)
+    eng.close()
+
+
+def test_auto_resident_chunks_fit_free_memory():
+    free, _ = torch.cuda.mem_get_info()
+    n = rm.CompactEngine.auto_resident_chunks(10_000_000, 2048, 1 << 20, 3)
+    assert 0 <= n <= 10 and (n + 3) * ((10_000_000 // 10 + 5) * 2048) <= free
