@@ -8,7 +8,12 @@
  *   - device pointers are plain CUDA device addresses owned by the caller;
  *     an engine owns only its own workspace;
  *   - `stream` is a cudaStream_t (NULL = the legacy default stream); every
- *     device call is stream-ordered and returns without synchronizing;
+ *     device call is stream-ordered and returns without synchronizing unless
+ *     its comment says otherwise (the device FASTA reader learns its record
+ *     counts on the host; destroying an engine waits for its work);
+ *   - an engine or reader handle serves one thread at a time (its workspace,
+ *     events and rebound tensor maps are per handle); different handles may
+ *     be used from different threads and streams concurrently;
  *   - index conventions follow the reference: global column ids are 1-based,
  *     0 marks an empty slot whose value is -Inf.
  *

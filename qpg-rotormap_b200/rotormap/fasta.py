@@ -10,6 +10,7 @@ from __future__ import annotations
 import ctypes
 import mmap
 import os
+import threading
 from collections.abc import Sequence
 from dataclasses import dataclass
 
@@ -150,16 +151,20 @@ class DeviceFastaFragments:
         return len(self.heads)
 
 
-_PINNED: dict = {}
+_PINNED = threading.local()
 
 
 def _pinned(tag: str, nbytes: int):
-    """A grow-only pinned host buffer per tag (callers synchronise before reuse)."""
+    """A grow-only pinned host buffer per tag and thread (the caller
+    synchronises its stream before the buffer is reused)."""
     import torch
-    buf = _PINNED.get(tag)
+    bufs = getattr(_PINNED, "bufs", None)
+    if bufs is None:
+        bufs = _PINNED.bufs = {}
+    buf = bufs.get(tag)
     if buf is None or buf.numel() < nbytes:
         buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, pin_memory=True)
-        _PINNED[tag] = buf
+        bufs[tag] = buf
     return buf[:nbytes]
 
 
