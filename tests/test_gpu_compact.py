@@ -100,8 +100,9 @@ def test_ring_rejects_bad_arguments():
 
 
 def test_compact_stream_ring_equals_resident(tmp_path):
-    """rope_topk_stream_compact: the host ring (resident = False) and the
-    uploaded index (resident = True) yield the same batches."""
+    """rope_topk_stream_compact: the uploaded index (resident = True), the
+    host ring streaming every chunk (resident_chunks = 0) and the ring
+    keeping what fits (the default "auto") yield the same batches."""
     from rotormap import synth
     heads = [">c1", ">c2"]
     recs = synth.random_genome([60_000, 40_000], seed=4)
@@ -115,10 +116,13 @@ def test_compact_stream_ring_equals_resident(tmp_path):
     a = list(rm.rope_topk_stream_compact(re, str(p), Bh, k=20, batch_size=128, score="scaled", scaleB=sb,
                                          resident=True))
     b = list(rm.rope_topk_stream_compact(re, str(p), Bh, k=20, batch_size=128, score="scaled", scaleB=sb,
-                                         resident=False, chunk_cols=2048))
-    assert [x.heads for x in a] == [x.heads for x in b]
-    for x, y in zip(a, b):
+                                         resident=False, chunk_cols=2048, resident_chunks=0))
+    c = list(rm.rope_topk_stream_compact(re, str(p), Bh, k=20, batch_size=128, score="scaled", scaleB=sb,
+                                         resident=False, chunk_cols=2048, resident_chunks="auto"))
+    assert [x.heads for x in a] == [x.heads for x in b] == [x.heads for x in c]
+    for x, y, z in zip(a, b, c):
         assert np.array_equal(x.vals, y.vals) and np.array_equal(x.locs, y.locs)
+        assert np.array_equal(x.vals, z.vals) and np.array_equal(x.locs, z.locs)
 
 
 @pytest.mark.parametrize("nres,depth", [(1, 2), (2, 2), (3, 3), (5, 2), (9, 2), (0, 2)])
