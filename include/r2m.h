@@ -127,9 +127,9 @@ typedef struct {
                       of every r2m_batch_gemm_topk (see r2m_engine_kernel_ms);
                       reserved[1]: kernel, 0 auto (CTA pairs above 128 reads),
                       1 single-CTA, 2 CTA-pair;
-                      reserved[2]: CTA-pair epilogue, 0 auto (8 warps for
-                      work units of at most 8192 column tiles, else 4),
-                      1 four warps, 2 eight warps (k <= 32) */
+                      reserved[2]: epilogue form of either kernel, 0 auto
+                      (8 warps for work units of at most 8192 column tiles,
+                      else 4), 1 four warps, 2 eight warps (k <= 32) */
 } r2m_tuning;
 
 /* Replaces TopKEngine(B; k, w, rows_cap, segs, engine, cout)

@@ -40,10 +40,22 @@ constexpr int BK = 128;           // K bytes per stage (one 128-byte swizzle row
 constexpr int STAGES = 4;
 constexpr int A_STAGE = BM * BK;  // 16 KiB
 constexpr int B_STAGE = BN * BK;  // 32 KiB
-constexpr int THREADS = 192;
 constexpr int TMEM_COLS = 512;
 constexpr long long WAIT_LIMIT = 4000000000LL;  // clock cycles (~2 s)
 constexpr int MAX_SPLITS = 128;
+// Epilogue forms of both kernels: 4 * H epilogue warps.  With H = 2 two warps
+// share each TMEM lane quarter, each draining one half (128 columns) of
+// every tile into its own reservoir, so a (read tile, column split) unit
+// leaves two partial lists per row.  That halves the per-warp latency chain
+// of a tile and the reservoir warm-up at every unit start -- the gain of short
+// units -- but keeps more warps busy, which under the board's power cap
+// lowers the clock of long units; the host picks H per launch
+// (epi_halves_for).  KT = 64 always uses H = 1 (its reservoir needs the
+// registers).
+__host__ __device__ constexpr int epi_threads(int H) { return 64 + 128 * H; }
+constexpr int SCRATCH_F = 17;  // floats per epilogue thread (16-value slow-path passes)
+// 256-column tiles per work unit at or below which the 8-warp epilogue pays
+constexpr int SHORT_UNIT_TILES = 8192;
 
 struct GemmArgs {
   int nb;
@@ -106,8 +118,8 @@ struct Reservoir {
   __device__ __forceinline__ void sort_desc() {}
 };
 
-template <int KT>
-__global__ void __launch_bounds__(THREADS, 1)
+template <int KT, int H>
+__global__ void __launch_bounds__(epi_threads(H), 1)
     k_gemm_topk(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -122,7 +134,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t *drain = acc_empty + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // 128 x 33 floats
+  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // epilogue threads x SCRATCH_F floats
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
@@ -134,7 +146,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&acc_full[a], 1);
-      mbar_init(&acc_empty[a], 4);
+      mbar_init(&acc_empty[a], 4 * H);  // epilogue warps
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -258,9 +270,11 @@ __global__ void __launch_bounds__(THREADS, 1)
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (top-k)
-    const int quarter = warp & 3;  // TMEM lanes [32*quarter, 32*quarter+32)
+    constexpr int CH = BN / 32 / H;  // 32-column chunks per warp and tile
+    const int quarter = warp & 3;    // TMEM lanes [32*quarter, 32*quarter+32)
+    const int half = (warp - 2) >> 2;  // tile chunks [CH half, CH half + CH)
     const int row_in_tile = quarter * 32 + lane;
-    float *scratch = scratch_all + (threadIdx.x - 64) * 33;
+    float *scratch = scratch_all + (threadIdx.x - 64) * SCRATCH_F;
     const bool f16 = g.score_mode == R2M_SCORE_F16;
     const bool scaled = g.score_mode == R2M_SCORE_SCALED;
     int acc = 0;
@@ -284,7 +298,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const long long colbase = (long long)t * BN;
         const bool tail = colbase + BN > g.N;
 #pragma unroll 1
-        for (int ch = 0; ch < BN / 32; ++ch) {
+        for (int ch = half * CH; ch < (half + 1) * CH; ++ch) {
           float v[32];
           __syncwarp();
           tmem_ld32(taddr + ch * 32, v);
@@ -316,14 +330,18 @@ __global__ void __launch_bounds__(THREADS, 1)
           for (int j = 1; j < 32; ++j) mx = fmaxf(mx, v[j]);
           if (f16) mx = round_f16(mx);
           if (mx > R.thr) {
-            // rare path: stage the chunk and insert its survivors one by one
+            // rare path: stage the chunk (16 values at a time) and insert its
+            // survivors one by one
 #pragma unroll
-            for (int j = 0; j < 32; ++j) scratch[j] = v[j];
+            for (int p = 0; p < 2; ++p) {
+#pragma unroll
+              for (int j = 0; j < 16; ++j) scratch[j] = v[16 * p + j];
 #pragma unroll 1
-            for (int j = 0; j < 32; ++j) {
-              float x = scratch[j];
-              if (f16) x = round_f16(x);
-              if (x > R.thr) R.insert(x, (int)(c0 + j));
+              for (int j = 0; j < 16; ++j) {
+                float x = scratch[j];
+                if (f16) x = round_f16(x);
+                if (x > R.thr) R.insert(x, (int)(c0 + 16 * p + j));
+              }
             }
           }
         }
@@ -337,8 +355,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       R.sort_desc();
       const int row = mt * BM + row_in_tile;
       if (row < g.nb) {
-        float *pv = g.part_vals + ((size_t)sp * g.mpad + row) * KT;
-        int *pc = g.part_cols + ((size_t)sp * g.mpad + row) * KT;
+        const size_t list = (size_t)sp * H + half;
+        float *pv = g.part_vals + (list * g.mpad + row) * KT;
+        int *pc = g.part_cols + (list * g.mpad + row) * KT;
 #pragma unroll
         for (int j = 0; j < KT; ++j) {
           pv[j] = R.v[j];
@@ -370,22 +389,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 // multicast is used anywhere.
 constexpr int STAGES2 = 6;
 constexpr int HALF_TILE = 128 * BK;  // 16 KiB
-// CTA-pair kernel: TMA warp, MMA warp and 4 * H epilogue warps.  With H = 2
-// two warps share each TMEM lane quarter, each draining one half (128
-// columns) of every tile into its own reservoir, so a (read tile, column
-// split) unit leaves two partial lists per row.  That halves the per-warp
-// latency chain of a tile and the reservoir warm-up at every unit start --
-// the gain of short units -- but keeps more warps busy, which under the
-// board's power cap lowers the clock of long units; the host picks H per
-// launch (pair_halves_for).  KT = 64 always uses H = 1 (its reservoir needs
-// the registers).
-__host__ __device__ constexpr int pair_threads(int H) { return 64 + 128 * H; }
-constexpr int SCRATCH2 = 17;  // floats per epilogue thread (16-value slow-path passes)
-// 256-column tiles per work unit at or below which the 8-warp epilogue pays
-constexpr int SHORT_UNIT_TILES = 8192;
-
+// CTA-pair kernel: TMA warp, MMA warp and 4 * H epilogue warps (epilogue
+// forms above).
 template <int KT, int H>
-__global__ void __launch_bounds__(pair_threads(H), 1)
+__global__ void __launch_bounds__(epi_threads(H), 1)
     k_gemm_topk2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem =
@@ -399,7 +406,7 @@ __global__ void __launch_bounds__(pair_threads(H), 1)
   uint64_t *drain = acc_empty + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // epilogue threads x SCRATCH2 floats
+  float *scratch_all = reinterpret_cast<float *>(tmem_slot + 4);  // epilogue threads x SCRATCH_F floats
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
@@ -544,7 +551,7 @@ __global__ void __launch_bounds__(pair_threads(H), 1)
     const int quarter = warp & 3;          // TMEM lanes this warp may read
     const int half = (warp - 2) >> 2;      // tile chunks [CH half, CH half + CH)
     const int row_in_tile = quarter * 32 + lane;
-    float *scratch = scratch_all + (threadIdx.x - 64) * SCRATCH2;
+    float *scratch = scratch_all + (threadIdx.x - 64) * SCRATCH_F;
     const bool f16 = g.score_mode == R2M_SCORE_F16;
     const bool scaled = g.score_mode == R2M_SCORE_SCALED;
     int acc = 0;
@@ -767,9 +774,9 @@ static int pick_kt(int k) {
   return 64;
 }
 
-static size_t gemm_smem_bytes() {
+static size_t gemm_smem_bytes(int H) {
   return 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + (2 * STAGES + 5) * 8 + 16 +
-         (size_t)BM * 33 * sizeof(float);
+         (size_t)(epi_threads(H) - 64) * SCRATCH_F * sizeof(float);
 }
 
 // Column splits for a given number of read tiles: enough units to keep
@@ -799,24 +806,24 @@ static int choose_splits(int m_tiles, int n_tiles, int ctas, int forced, int max
   return best;
 }
 
-template <int KT>
+template <int KT, int H>
 static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmArgs &g, int ctas,
                        cudaStream_t st) {
-  size_t smem = gemm_smem_bytes();
+  size_t smem = gemm_smem_bytes(H);
   // a function attribute is per device: set it on every launch (cheap)
-  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_gemm_topk<KT><<<ctas, THREADS, smem, st>>>(mA, mB, g);
+  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk<KT, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_gemm_topk<KT, H><<<ctas, epi_threads(H), smem, st>>>(mA, mB, g);
   R2M_CUDA(cudaGetLastError());
   return R2M_OK;
 }
 
 static size_t gemm2_smem_bytes(int H) {
   return 1024 + (size_t)STAGES2 * 2 * HALF_TILE + (2 * STAGES2 + 5) * 8 + 16 +
-         (size_t)(pair_threads(H) - 64) * SCRATCH2 * sizeof(float);
+         (size_t)(epi_threads(H) - 64) * SCRATCH_F * sizeof(float);
 }
 
 // Epilogue halves for a pair-kernel launch: 2 for short units (k <= 32).
-static int pair_halves_for(int KT, int n_tiles, int splits) {
+static int epi_halves_for(int KT, int n_tiles, int splits) {
   return (KT <= 32 && (n_tiles + splits - 1) / splits <= SHORT_UNIT_TILES) ? 2 : 1;
 }
 
@@ -827,7 +834,7 @@ static int launch_gemm2(const CUtensorMap &mA, const CUtensorMap &mB, const Gemm
   R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk2<KT, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(2 * pairs, 1, 1);
-  cfg.blockDim = dim3(pair_threads(H), 1, 1);
+  cfg.blockDim = dim3(epi_threads(H), 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -858,8 +865,9 @@ static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int 
     int tile = kind == 2 ? 256 : BM;
     int mt = (h + tile - 1) / tile;
     int c = kind == 2 ? (ctas / 2 > 0 ? ctas / 2 : 1) : ctas;
-    // the pair kernel may leave two partial lists per row and split
-    const int H = (kind == 2 && KT <= 32) ? 2 : 1;
+    // either kernel may leave two partial lists per row and split
+    (void)kind;
+    const int H = KT <= 32 ? 2 : 1;
     size_t l = (size_t)choose_splits(mt, n_tiles, c, forced, MAX_SPLITS / H) * H * mt * tile;
     if (l > lists) lists = l;
   }
@@ -1056,11 +1064,10 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   g.num_m_tiles = (nb + tile - 1) / tile;
   g.N = eng->N;
   g.n_tiles = eng->n_tiles;
-  const int hmax = (kind == 2 && eng->KT <= 32) ? 2 : 1;
+  const int hmax = eng->KT <= 32 ? 2 : 1;
   g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / hmax);
-  int halves = 1;
-  if (kind == 2)
-    halves = eng->epi == 1 ? 1 : eng->epi == 2 ? hmax : pair_halves_for(eng->KT, eng->n_tiles, g.splits);
+  const int halves =
+      eng->epi == 1 ? 1 : eng->epi == 2 ? hmax : epi_halves_for(eng->KT, eng->n_tiles, g.splits);
   const int lists_per_row = halves * g.splits;  // partial lists each row leaves
   g.num_kb = (eng->rdim + BK - 1) / BK;
   g.score_mode = eng->score_mode;
@@ -1092,12 +1099,21 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
       }
     }
   } else {
-    switch (eng->KT) {
-      case 8: rc = launch_gemm<8>(mapA, eng->mapB, g, ctas, st); break;
-      case 16: rc = launch_gemm<16>(mapA, eng->mapB, g, ctas, st); break;
-      case 20: rc = launch_gemm<20>(mapA, eng->mapB, g, ctas, st); break;
-      case 32: rc = launch_gemm<32>(mapA, eng->mapB, g, ctas, st); break;
-      default: rc = launch_gemm<64>(mapA, eng->mapB, g, ctas, st); break;
+    if (halves == 2) {
+      switch (eng->KT) {
+        case 8: rc = launch_gemm<8, 2>(mapA, eng->mapB, g, ctas, st); break;
+        case 16: rc = launch_gemm<16, 2>(mapA, eng->mapB, g, ctas, st); break;
+        case 20: rc = launch_gemm<20, 2>(mapA, eng->mapB, g, ctas, st); break;
+        default: rc = launch_gemm<32, 2>(mapA, eng->mapB, g, ctas, st); break;
+      }
+    } else {
+      switch (eng->KT) {
+        case 8: rc = launch_gemm<8, 1>(mapA, eng->mapB, g, ctas, st); break;
+        case 16: rc = launch_gemm<16, 1>(mapA, eng->mapB, g, ctas, st); break;
+        case 20: rc = launch_gemm<20, 1>(mapA, eng->mapB, g, ctas, st); break;
+        case 32: rc = launch_gemm<32, 1>(mapA, eng->mapB, g, ctas, st); break;
+        default: rc = launch_gemm<64, 1>(mapA, eng->mapB, g, ctas, st); break;
+      }
     }
   }
   if (rc) return rc;
@@ -1236,11 +1252,11 @@ extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_sc
   long long units = (long long)m_tiles * splits;
   int ctas = (int)(units < ctas_max ? units : ctas_max);
   switch (KT) {
-    case 8: rc = launch_gemm<8>(mapA, mapB, g, ctas, st); break;
-    case 16: rc = launch_gemm<16>(mapA, mapB, g, ctas, st); break;
-    case 20: rc = launch_gemm<20>(mapA, mapB, g, ctas, st); break;
-    case 32: rc = launch_gemm<32>(mapA, mapB, g, ctas, st); break;
-    default: rc = launch_gemm<64>(mapA, mapB, g, ctas, st); break;
+    case 8: rc = launch_gemm<8, 1>(mapA, mapB, g, ctas, st); break;
+    case 16: rc = launch_gemm<16, 1>(mapA, mapB, g, ctas, st); break;
+    case 20: rc = launch_gemm<20, 1>(mapA, mapB, g, ctas, st); break;
+    case 32: rc = launch_gemm<32, 1>(mapA, mapB, g, ctas, st); break;
+    default: rc = launch_gemm<64, 1>(mapA, mapB, g, ctas, st); break;
   }
   if (rc) return rc;
   const int warps = 8;

@@ -34,7 +34,7 @@ def bucket_rows(n: int) -> int:
 
 class Autotuner:
     """Picks (splits, ctas, epilogue) for an engine and row count by timing
-    candidates.  The CTA-pair epilogue form (4 or 8 warps) depends on how
+    candidates.  The epilogue form (4 or 8 warps) depends on how
     long a work unit is, so it is only tuned when the candidates run on the
     engine itself; on a proxy index the automatic rule stays."""
 
@@ -99,7 +99,7 @@ class Autotuner:
             ms = timed(s, c, "auto")
             if ms < best_ms:
                 best, best_ms = (s, c, "auto"), ms
-        if target is eng and rows > 128 and eng.k <= 32:  # the CTA-pair kernel's epilogue forms
+        if target is eng and eng.k <= 32:  # the fused kernels' two epilogue forms
             for ep in ("4", "8"):
                 ms = timed(best[0], best[1], ep)
                 if ms < best_ms:

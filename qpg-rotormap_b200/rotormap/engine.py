@@ -19,7 +19,8 @@ from .encoder import RopeEncoder, encode_frag_real_batch, f16_to_f8
 from .fasta import DeviceFastaFragments, FastaFragments, fasta_reads, fasta_reads_device
 
 _MODES = {"f16": _lib.SCORE_F16, "f32": _lib.SCORE_F32, "scaled": _lib.SCORE_SCALED}
-# CTA-pair epilogue: auto, 4 warps, or 8 warps (two column halves; k <= 32)
+# epilogue form of the fused kernels: auto, 4 warps, or 8 warps (two column
+# halves; k <= 32)
 _EPILOGUES = {"auto": 0, "4": 1, "8": 2}
 # fused kernel variant: one CTA per 128-read tile, or CTA pairs (cta_group::2)
 # per 256-read tile; "auto" uses pairs above 128 reads

@@ -147,20 +147,21 @@ def test_engine_rejects_bad_arguments():
 
 
 @pytest.mark.parametrize("score", ["f16", "scaled"])
-def test_pair_kernel_epilogue_forms_agree(score):
-    """The CTA-pair kernel drains tiles with 8 epilogue warps (two column
-    halves, two partial lists per row) when a work unit spans at most 8192
-    column tiles and with 4 warps otherwise; both forms give the same values,
-    locations and tie order.  One split over 8,600 tiles takes the 4-warp
-    form, two splits the 8-warp form."""
+@pytest.mark.parametrize("kernel", ["1sm", "2sm"])
+def test_pair_kernel_epilogue_forms_agree(score, kernel):
+    """Both kernels drain tiles with 8 epilogue warps (two column halves, two
+    partial lists per row) when a work unit spans at most 8192 column tiles
+    and with 4 warps otherwise; both forms give the same values, locations
+    and tie order.  One split over 8,600 tiles takes the 4-warp form, two
+    splits the 8-warp form."""
     rng = np.random.default_rng(77)
     nb, N, rdim = 300, 2_201_000, 16
     A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
     B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
     sa = rng.uniform(0.5, 2.0, nb).astype(np.float32) if score == "scaled" else None
     sb = rng.uniform(0.5, 2.0, N).astype(np.float32) if score == "scaled" else None
-    v1, l1 = run_engine(A8, B8, 20, score, sa, sb, splits=1, kernel="2sm")
-    v2, l2 = run_engine(A8, B8, 20, score, sa, sb, splits=2, kernel="2sm")
+    v1, l1 = run_engine(A8, B8, 20, score, sa, sb, splits=1, kernel=kernel)
+    v2, l2 = run_engine(A8, B8, 20, score, sa, sb, splits=2, kernel=kernel)
     assert np.array_equal(v1, v2) and np.array_equal(l1, l2)
     # spot-check against brute-force scores of a few rows
     from oracle import oracle as orc
@@ -172,7 +173,8 @@ def test_pair_kernel_epilogue_forms_agree(score):
 
 
 @pytest.mark.parametrize("k", [8, 20, 32, 64])
-def test_pair_kernel_forced_epilogue_forms(k):
+@pytest.mark.parametrize("kernel", ["1sm", "2sm"])
+def test_pair_kernel_forced_epilogue_forms(k, kernel):
     """Forcing 4 or 8 epilogue warps (k = 64 always runs 4) changes nothing
     in the results, across split counts."""
     rng = np.random.default_rng(k)
@@ -180,7 +182,7 @@ def test_pair_kernel_forced_epilogue_forms(k):
     A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
     B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
     A = torch.from_numpy(A8).cuda()
-    eng = rm.TopKEngine(torch.from_numpy(B8).cuda(), k=k, rows_cap=nb, kernel="2sm")
+    eng = rm.TopKEngine(torch.from_numpy(B8).cuda(), k=k, rows_cap=nb, kernel=kernel)
     ref = None
     for ep in ("4", "8", "auto"):
         for s in (1, 3, 17):
