@@ -349,6 +349,10 @@ typedef struct r2m_dreads r2m_dreads;
  * r2m_dreads_free. */
 int r2m_fasta_reads_device(const void *d_data, size_t len, int k, r2m_stream_t stream, r2m_dreads **out);
 int64_t r2m_dreads_count(const r2m_dreads *r);
+/* 1 when a record whose header line is not closed ended the parse (that
+ * record and everything after it dropped), else 0 -- a caller that feeds a
+ * file in pieces cut at record starts stops after such a piece. */
+int r2m_dreads_stopped(const r2m_dreads *r);
 /* device, r2m_dreads_count(r) x cld(k,16) words */
 const uint32_t *r2m_dreads_words(const r2m_dreads *r);
 /* device, r2m_dreads_count(r) x 2 int64 header byte spans */

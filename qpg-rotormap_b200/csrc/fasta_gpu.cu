@@ -48,6 +48,7 @@ struct r2m_dreads {
   int64_t *spans = nullptr;   // n x 2: header [start, end) byte offsets
   uint8_t *heads = nullptr;   // every header followed by '\n'
   size_t head_bytes = 0;
+  bool stopped = false;  // an unclosed header ended the parse
   cudaStream_t stream = nullptr;
 };
 
@@ -561,6 +562,7 @@ extern "C" int r2m_fasta_reads_device(const void *d_data, size_t len, int k, r2m
       return bail(e, "kept count");
     const int64_t Kc = tot[0], cut = std::min<int64_t>(tot[2], R);
     res->n = Kc;
+    res->stopped = cut < R;
     res->head_bytes = (size_t)tot[1];
     if (Kc > 0) {
       const bool all_kept = Kc == cut;  // slot order is already the rank order
@@ -595,6 +597,8 @@ extern "C" int r2m_fasta_reads_device(const void *d_data, size_t len, int k, r2m
 }
 
 extern "C" int64_t r2m_dreads_count(const r2m_dreads *r) { return r ? r->n : 0; }
+
+extern "C" int r2m_dreads_stopped(const r2m_dreads *r) { return r && r->stopped ? 1 : 0; }
 
 extern "C" const uint32_t *r2m_dreads_words(const r2m_dreads *r) { return r ? r->words : nullptr; }
 

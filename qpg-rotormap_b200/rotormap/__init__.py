@@ -9,7 +9,8 @@ from .encoder import (RopeEncoder, dim, encode_frag_real_batch, encode_frag_real
                       f16_to_f8, f32_to_f8, revcomp_frag_words)
 from .engine import (CompactEngine, Mapper, PlainEngine, TopKBatch, TopKEngine, batch_gemm_topk, padmul, resident_fits,
                      rope_topk_stream, rope_topk_stream_compact, topk_flow, upload_fp16_as_f8)
-from .fasta import DeviceFastaFragments, FastaFragments, HeaderList, fasta_reads, fasta_reads_device
+from .fasta import (DeviceFastaFragments, FastaFragments, HeaderList, fasta_chunks_device, fasta_reads,
+                    fasta_reads_device)
 from .index import (FP8_FORMAT, SCALED_FORMAT, Index, RefPack, build_index, build_index_packed,
                     index_database,
                     load_index, pack_records, pack_reference, save_index, window_positions)

@@ -87,6 +87,7 @@ SIGNATURES = [
     ("r2m_genome_free", None, [P]),
     ("r2m_fasta_reads_device", I, [P, SZ, I, P, ctypes.POINTER(P)]),
     ("r2m_dreads_count", I64, [P]),
+    ("r2m_dreads_stopped", I, [P]),
     ("r2m_dreads_words", P, [P]),
     ("r2m_dreads_spans", P, [P]),
     ("r2m_dreads_header_blob", P, [P, ctypes.POINTER(SZ)]),

@@ -16,7 +16,7 @@ import torch
 from . import _lib
 from ._lib import Tuning, check, lib, ptr, stream_handle
 from .encoder import RopeEncoder, encode_frag_real_batch, f16_to_f8
-from .fasta import DeviceFastaFragments, FastaFragments, fasta_reads, fasta_reads_device
+from .fasta import DeviceFastaFragments, FastaFragments, fasta_chunks_device, fasta_reads, fasta_reads_device
 
 _MODES = {"f16": _lib.SCORE_F16, "f32": _lib.SCORE_F32, "scaled": _lib.SCORE_SCALED}
 # epilogue form of the fused kernels: auto, 4 warps, or 8 warps (two column
@@ -392,6 +392,15 @@ def _batches(frags: FastaFragments | DeviceFastaFragments, batch_size: int):
         yield b0, frags.words[b0:b0 + batch_size], frags.heads[b0:b0 + batch_size]
 
 
+def _chunked_batches(pieces, batch_size: int):
+    """Batches over consecutive reader pieces, numbered across the input."""
+    first0 = 0
+    for frags in pieces:
+        for b0, words, heads in _batches(frags, batch_size):
+            yield first0 + b0, words, heads
+        first0 += len(frags)
+
+
 def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stream=None):
     """topk_flow (engine_fp8.jl:498-547) over an iterable of
     (first0, words (nb, W), heads) batches -- words as host uint32 arrays or
@@ -431,23 +440,26 @@ def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int
                      batch_size: int = 8192, rows_cap: int | None = None, normalize: int = 0,
                      score: str = "f16", scaleB: torch.Tensor | None = None, parts: int | None = None,
                      segs: int | None = None, engine: TopKEngine | None = None, stream=None,
-                     reader: str = "device"):
+                     reader: str = "device", chunk_bytes: int = 1 << 30):
     """rope_topk_stream (engine_fp8.jl:576-594): FASTA -> encode -> fp8 GEMM +
     top-k against the resident B -> TopKBatch per batch (file order).
 
-    reader = "device" parses the FASTA on the GPU (the words stay in HBM);
-    "host" uses the native host reader with `parts` threads.  Both give the
-    same reads."""
+    reader = "device" parses the FASTA on the GPU (the words stay in HBM),
+    `chunk_bytes` of the file at a time (cut at record starts), so inputs of
+    any size stream through bounded memory; "host" uses the native host
+    reader with `parts` threads on the whole input.  Both give the same
+    reads."""
     if B.shape[1] != re.rdim:
         raise ValueError(f"B is {tuple(B.shape)}; the encoder's real embedding dim is {re.rdim}")
     if reader == "device":
-        frags = fasta_reads_device(file, k=re.k, device=B.device, stream=stream)
+        source = _chunked_batches(fasta_chunks_device(file, k=re.k, chunk_bytes=chunk_bytes, device=B.device,
+                                                      stream=stream), batch_size)
     elif reader == "host":
-        frags = fasta_reads(file, k=re.k, parts=parts)
+        source = _batches(fasta_reads(file, k=re.k, parts=parts), batch_size)
     else:
         raise ValueError('reader must be "device" or "host"')
     eng = engine or TopKEngine(B, k=k, rows_cap=rows_cap or batch_size, score=score, scaleB=scaleB)
-    yield from topk_flow(_batches(frags, batch_size), eng, re, normalize, stream)
+    yield from topk_flow(source, eng, re, normalize, stream)
 
 
 def resident_need(host_bytes: int, rows_cap: int, rdim: int, k: int = 20) -> int:
@@ -498,11 +510,12 @@ def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size:
                         pin=pin, resident_chunks=resident_chunks)
     try:
         if reader == "device":
-            frags = fasta_reads_device(file, k=re.k, device=eng.device, stream=stream)
+            source = _chunked_batches(fasta_chunks_device(file, k=re.k, device=eng.device, stream=stream),
+                                      batch_size)
         elif reader == "host":
-            frags = fasta_reads(file, k=re.k, parts=parts)
+            source = _batches(fasta_reads(file, k=re.k, parts=parts), batch_size)
         else:
             raise ValueError('reader must be "device" or "host"')
-        yield from topk_flow(_batches(frags, batch_size), eng, re, normalize, stream)
+        yield from topk_flow(source, eng, re, normalize, stream)
     finally:
         eng.close()

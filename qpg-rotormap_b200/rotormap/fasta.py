@@ -146,6 +146,7 @@ class DeviceFastaFragments:
     k: int
     words: "torch.Tensor"
     heads: Sequence
+    stopped: bool = False  # an unclosed header ended the parse
 
     def __len__(self) -> int:
         return len(self.heads)
@@ -216,6 +217,7 @@ def fasta_reads_device(src, k: int = 20_000, device=None, stream=None) -> Device
         check(L.r2m_fasta_reads_device(ptr(dev_bytes) if n else None, n, k, stream_handle(st), ctypes.byref(handle)))
         try:
             cnt = int(L.r2m_dreads_count(handle))
+            stopped = bool(L.r2m_dreads_stopped(handle))
             W = (k + 15) // 16
             words = torch.empty((cnt, W), dtype=torch.int32, device=dev)
             heads = HeaderList(b"", [0])
@@ -230,20 +232,57 @@ def fasta_reads_device(src, k: int = 20_000, device=None, stream=None) -> Device
         finally:
             st.synchronize()
             L.r2m_dreads_free(handle)
-    return DeviceFastaFragments(k, words, heads)
+    return DeviceFastaFragments(k, words, heads, stopped)
 
 
-def _wrap_device(addr: int, count: int, dtype, dev):
-    """A torch view of `count` elements of library-owned device memory."""
-    import torch
+def _last_record_start(buf: bytes) -> int:
+    """Offset of the last record start after offset 0 (a '>' that follows
+    '\n' or '\r'), or -1."""
+    i = max(buf.rfind(b"\n>"), buf.rfind(b"\r>"))
+    return i + 1 if i >= 0 else -1
 
-    class _Cai:
-        __cuda_array_interface__ = {
-            "shape": (count,),
-            "typestr": {torch.int32: "<i4", torch.int64: "<i8", torch.uint8: "|u1"}[dtype],
-            "data": (addr, False),
-            "version": 3,
-            "strides": None,
-        }
 
-    return torch.as_tensor(_Cai(), device=dev)
+def _fasta_pieces(src, chunk_bytes: int):
+    """The input (bytes or a path) in pieces of about `chunk_bytes`, each cut
+    at its last record start (the rest carries over); a piece that holds no
+    record start after its first byte grows until one appears or the input
+    ends.  The pieces concatenate to the input and no record spans two."""
+    import io as _io
+    if chunk_bytes < 1:
+        raise ValueError("chunk_bytes must be >= 1")
+    f = _io.BytesIO(bytes(src)) if isinstance(src, (bytes, bytearray, memoryview)) else open(os.fspath(src), "rb")
+    try:
+        carry = b""
+        while True:
+            block = f.read(chunk_bytes)
+            eof = len(block) < chunk_bytes
+            data = carry + block if carry else block
+            if not eof:
+                cut = _last_record_start(data)
+                if cut <= 0:  # no record start after the first byte yet: read on
+                    carry = data
+                    continue
+                piece, carry = data[:cut], data[cut:]
+            else:
+                piece, carry = data, b""
+            if piece:
+                yield piece
+            if eof:
+                return
+    finally:
+        f.close()
+
+
+def fasta_chunks_device(src, k: int = 20_000, chunk_bytes: int = 1 << 30, device=None, stream=None):
+    """fasta_reads on the GPU for inputs of any size: the file (or bytes) is
+    read in blocks of about `chunk_bytes`, each cut at its last record start
+    (the rest carries over to the next block), and every piece is parsed by
+    fasta_reads_device.  Pieces never split a record, so the records, words
+    and headers are those of the whole input; after a piece in which an
+    unclosed header ended the parse, nothing further is read (the rule of
+    the whole-input reader).  Yields DeviceFastaFragments in file order."""
+    for piece in _fasta_pieces(src, chunk_bytes):
+        frags = fasta_reads_device(piece, k=k, device=device, stream=stream)
+        yield frags
+        if frags.stopped:
+            return

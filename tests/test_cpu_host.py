@@ -345,3 +345,32 @@ def test_header_list_behaves_like_a_list():
         hl[5]
     f = rm.fasta_reads(b">r1 x\nACGT\n>r2\nAAAA\n", k=4)
     assert isinstance(f.heads, rm.HeaderList) and f.heads == [">r1 x", ">r2"]
+
+
+@pytest.mark.parametrize("chunk", [1, 7, 64, 1000, 1 << 20])
+def test_fasta_pieces_cut_at_record_starts(chunk):
+    """The chunked readers' pieces: they concatenate to the input, every
+    piece after the first starts a record, and parsing piece by piece gives
+    the whole input's records (host reader; inputs without an unclosed
+    header, where the two parses cannot differ)."""
+    from rotormap.fasta import _fasta_pieces
+    rng = np.random.default_rng(chunk)
+    recs = []
+    for r in range(60):
+        n = int(rng.integers(0, 300))
+        seq = synth.LETTERS[rng.integers(0, 4, n)].tobytes()
+        eol = [b"\n", b"\r\n"][int(rng.integers(0, 2))]
+        w = int(rng.integers(1, 90))
+        recs.append(b">rec%d x>y\n" % r + eol.join(seq[i:i + w] for i in range(0, n, w)) + eol)
+    raw = b"junk > line\n" + b"".join(recs)
+    pieces = list(_fasta_pieces(raw, chunk))
+    assert b"".join(pieces) == raw
+    for p in pieces[1:]:
+        assert p.startswith(b">")
+    for k in (1, 100):
+        whole = rm.fasta_reads(raw, k=k)
+        parts = [rm.fasta_reads(p, k=k) for p in pieces]
+        assert [h for f in parts for h in f.heads] == list(whole.heads)
+        got = [f.words for f in parts if len(f)]
+        assert np.array_equal(np.concatenate(got) if got else np.zeros((0, whole.words.shape[1]), np.uint32),
+                              whole.words)

@@ -124,3 +124,43 @@ def test_device_reader_rejects_bad_arguments():
     with pytest.raises(ValueError):
         rm.fasta_reads_device(torch.zeros(4, dtype=torch.int32, device="cuda"), k=4)
     assert len(rm.fasta_reads_device(b"", k=4)) == 0
+
+
+@pytest.mark.parametrize("chunk", [50, 999, 10_000, 1 << 30])
+def test_device_reader_in_pieces_equals_whole_input(chunk):
+    """fasta_chunks_device (the file in pieces cut at record starts) yields
+    the whole-input records, and stops at an unclosed header exactly where
+    the whole-input reader does."""
+    rng = np.random.default_rng(chunk % 1000)
+    recs = []
+    for r in range(400):
+        n = int(rng.integers(100, 200))
+        seq = synth.LETTERS[rng.integers(0, 4, n)].tobytes()
+        eol = [b"\n", b"\r\n"][int(rng.integers(0, 2))]
+        recs.append(b">r%d\n" % r + seq[:70] + eol + seq[70:] + eol)
+    for raw in (b"".join(recs), b"".join(recs[:250]) + b">open\r" + b"".join(recs[250:])):
+        whole = rm.fasta_reads_device(raw, k=120)
+        pieces = list(rm.fasta_chunks_device(raw, k=120, chunk_bytes=chunk))
+        assert [h for p in pieces for h in p.heads] == list(whole.heads)
+        assert torch.equal(torch.cat([p.words for p in pieces]), whole.words)
+        assert pieces[-1].stopped == whole.stopped
+
+
+def test_stream_in_small_pieces_equals_host_reader(tmp_path):
+    """rope_topk_stream over a file read in small pieces: the same batches
+    (numbering included) as the whole-input host reader."""
+    heads = [">g1"]
+    recs = synth.random_genome([40_000], seed=3)
+    re = rm.RopeEncoder(k=150, s=8, m=4, c=4)
+    idx = rm.build_index(re, synth.genome_fasta(heads, recs), kstep=15)
+    reads, hd, _, _ = synth.sample_reads_even(heads, recs, 500, 150, 0.05, seed=9)
+    p = tmp_path / "r.fa"
+    p.write_bytes(synth.reads_fasta(hd, reads))
+    a = list(rm.rope_topk_stream(re, str(p), idx.embeds8, k=20, batch_size=128, reader="device", chunk_bytes=7000))
+    b = list(rm.rope_topk_stream(re, str(p), idx.embeds8, k=20, batch_size=128, reader="host"))
+    assert [h for x in a for h in x.heads] == [h for x in b for h in x.heads] == hd
+    va = np.concatenate([x.vals for x in a]); vb = np.concatenate([x.vals for x in b])
+    la = np.concatenate([x.locs for x in a]); lb = np.concatenate([x.locs for x in b])
+    assert np.array_equal(va, vb) and np.array_equal(la, lb)
+    firsts = [x.first for x in a]
+    assert firsts[0] == 1 and all(f2 - f1 == len(x.heads) for f1, f2, x in zip(firsts, firsts[1:], a))
