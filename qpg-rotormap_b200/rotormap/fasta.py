@@ -286,3 +286,19 @@ def fasta_chunks_device(src, k: int = 20_000, chunk_bytes: int = 1 << 30, device
         yield frags
         if frags.stopped:
             return
+
+
+def _wrap_device(addr: int, count: int, dtype, dev):
+    """A torch view of `count` elements of library-owned device memory."""
+    import torch
+
+    class _Cai:
+        __cuda_array_interface__ = {
+            "shape": (count,),
+            "typestr": {torch.int32: "<i4", torch.int64: "<i8", torch.uint8: "|u1"}[dtype],
+            "data": (addr, False),
+            "version": 3,
+            "strides": None,
+        }
+
+    return torch.as_tensor(_Cai(), device=dev)

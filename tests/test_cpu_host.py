@@ -374,3 +374,33 @@ def test_fasta_pieces_cut_at_record_starts(chunk):
         got = [f.words for f in parts if len(f)]
         assert np.array_equal(np.concatenate(got) if got else np.zeros((0, whole.words.shape[1]), np.uint32),
                               whole.words)
+
+
+def test_package_modules_bind_every_name_they_load():
+    """A static check of the host package (and bench.py): every name a
+    module reads is bound somewhere in it (definition, import, assignment,
+    argument) or is a builtin -- GPU-only code paths are covered too."""
+    import ast
+    import builtins
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    paths = sorted((root / "qpg-rotormap_b200" / "rotormap").glob("*.py")) + [root / "bench.py"]
+    for path in paths:
+        t = ast.parse(path.read_text())
+        bound = set()
+        for x in ast.walk(t):
+            if isinstance(x, ast.Name) and isinstance(x.ctx, (ast.Store, ast.Del)):
+                bound.add(x.id)
+            elif isinstance(x, (ast.FunctionDef, ast.AsyncFunctionDef, ast.ClassDef)):
+                bound.add(x.name)
+            elif isinstance(x, ast.arg):
+                bound.add(x.arg)
+            elif isinstance(x, (ast.Import, ast.ImportFrom)):
+                for a in x.names:
+                    bound.add((a.asname or a.name).split(".")[0])
+            elif isinstance(x, ast.ExceptHandler) and x.name:
+                bound.add(x.name)
+        used = {x.id for x in ast.walk(t) if isinstance(x, ast.Name) and isinstance(x.ctx, ast.Load)}
+        missing = sorted(u for u in used if u not in bound and not hasattr(builtins, u)
+                         and u not in ("__file__", "__name__"))
+        assert not missing, f"{path.name}: {missing}"
