@@ -241,6 +241,19 @@ int r2m_plain_batch_gemm_topk(r2m_plain_engine *eng, const uint8_t *d_A,
                               int nb, float *d_vals, int32_t *d_locs,
                               r2m_stream_t stream);
 
+/* ---------------------------------------------------------- top-k merge */
+
+/* The merge of a column-sharded search (one rank per index shard, each with
+ * its local top-k shifted to global 1-based columns, gathered side by side):
+ * d_vals / d_locs hold per row `lists` sorted lists of k entries, laid out
+ * [list 0 | list 1 | ...] (nb, lists*k); the row's top-kout under the
+ * engine's order (value descending, ties by ascending column; column 0 =
+ * empty, last) goes to (nb, kout).  lists <= 32.  Extends the reference's
+ * single-device merge (RotorMap/gemm/topk_kernels.jl:213-347) across
+ * devices; stream-ordered. */
+int r2m_merge_topk_lists(const float *d_vals, const int32_t *d_locs, int lists, int nb, int k, int kout,
+                         float *d_out_vals, int32_t *d_out_locs, r2m_stream_t stream);
+
 /* ----------------------------------------------------------- match table */
 
 typedef struct r2m_text r2m_text;

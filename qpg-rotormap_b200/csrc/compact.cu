@@ -27,6 +27,7 @@
 // than `depth`.  A search visits the chunks in column order, so the resident
 // ones are searched while the first streamed ones are in flight.
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -93,6 +94,53 @@ __global__ void k_merge_running(float *__restrict__ vals, int32_t *__restrict__ 
       locs[(size_t)r * k + t] = c_l[j] == 0 ? 0 : (int32_t)(c_l[j] + off);
       ++j;
     }
+  }
+}
+
+// Merge G sorted (value desc, column asc; empty = column 0) lists of k per
+// row, laid out row by row as [list 0 | list 1 | ...] (nb, G*k), into the
+// row's top-k.  One warp per row, one lane per list (G <= 32); k rounds of a
+// warp arg-max, ties by column then by list.
+__global__ void k_merge_lists(const float *__restrict__ vals, const int32_t *__restrict__ locs, int G, int nb,
+                              int k, int kout, float *__restrict__ out_v, int32_t *__restrict__ out_l) {
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= nb) return;
+  const unsigned FULL = 0xFFFFFFFFu;
+  const float *rv = vals + (size_t)row * G * k;
+  const int32_t *rl = locs + (size_t)row * G * k;
+  int head = 0;
+  auto load = [&](int h, float &v, int &c) {
+    if (lane < G && h < k && rl[lane * k + h] != 0) {
+      v = rv[lane * k + h];
+      c = rl[lane * k + h];
+    } else {
+      v = -INFINITY;
+      c = INT_MAX;
+    }
+  };
+  float hv;
+  int hc;
+  load(0, hv, hc);
+  for (int t = 0; t < kout; ++t) {
+    float wv = hv;
+    int wc = hc, wl = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(FULL, wv, o);
+      const int oc = __shfl_xor_sync(FULL, wc, o);
+      const int ol = __shfl_xor_sync(FULL, wl, o);
+      const bool better = (ov > wv) || (ov == wv && oc < wc) || (ov == wv && oc == wc && ol < wl);
+      wv = better ? ov : wv;
+      wc = better ? oc : wc;
+      wl = better ? ol : wl;
+    }
+    if (lane == 0) {
+      const bool empty = wc == INT_MAX;
+      out_v[(size_t)row * kout + t] = empty ? -INFINITY : wv;
+      out_l[(size_t)row * kout + t] = empty ? 0 : wc;
+    }
+    if (lane == wl) load(++head, hv, hc);
   }
 }
 
@@ -229,6 +277,20 @@ extern "C" int r2m_compact_destroy(r2m_compact *c) {
   if (!c) return R2M_OK;
   cudaDeviceSynchronize();
   destroy(c);
+  return R2M_OK;
+}
+
+extern "C" int r2m_merge_topk_lists(const float *d_vals, const int32_t *d_locs, int lists, int nb, int k,
+                                    int kout, float *d_out_vals, int32_t *d_out_locs, r2m_stream_t stream) {
+  R2M_REQUIRE(lists >= 1 && lists <= 32, "lists must be in 1..32");
+  R2M_REQUIRE(k >= 1 && kout >= 1 && kout <= lists * k, "need k >= 1 and 1 <= kout <= lists * k");
+  R2M_REQUIRE(nb >= 0, "nb must be >= 0");
+  if (nb == 0) return R2M_OK;
+  R2M_REQUIRE(d_vals && d_locs && d_out_vals && d_out_locs, "null pointer");
+  const int warps = 8;
+  k_merge_lists<<<(nb + warps - 1) / warps, 32 * warps, 0, as_stream(stream)>>>(d_vals, d_locs, lists, nb, k, kout,
+                                                                                 d_out_vals, d_out_locs);
+  R2M_CUDA(cudaGetLastError());
   return R2M_OK;
 }
 

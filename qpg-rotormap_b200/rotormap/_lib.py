@@ -74,6 +74,7 @@ SIGNATURES = [
     ("r2m_format_f32", I, [ctypes.c_float, ctypes.c_char_p, SZ]),
     ("r2m_compact_create", I, [P, P, I, I64, I, I, I, I64, I, I, I, P, ctypes.POINTER(P)]),
     ("r2m_compact_resident_chunks", I64, [P]),
+    ("r2m_merge_topk_lists", I, [P, P, I, I, I, I, P, P, P]),
     ("r2m_compact_destroy", I, [P]),
     ("r2m_compact_chunks", I64, [P]),
     ("r2m_compact_is_pinned", I, [P]),

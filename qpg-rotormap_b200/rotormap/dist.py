@@ -43,13 +43,40 @@ def merge_topk(vals: torch.Tensor, locs: torch.Tensor, k: int):
     return torch.gather(vals, 1, order), torch.gather(locs, 1, order)
 
 
+def merge_topk_lists(vals: torch.Tensor, locs: torch.Tensor, lists: int, k: int, stream=None):
+    """merge_topk of `lists` sorted k-lists per row laid side by side, on the
+    GPU with the library's merge kernel (r2m_merge_topk_lists)."""
+    from ._lib import check, lib, ptr, stream_handle
+    nb = vals.shape[0]
+    vals = vals.contiguous()
+    locs = locs.to(torch.int32).contiguous()
+    ov = torch.empty((nb, k), dtype=torch.float32, device=vals.device)
+    ol = torch.empty((nb, k), dtype=torch.int32, device=vals.device)
+    check(lib().r2m_merge_topk_lists(ptr(vals), ptr(locs), lists, nb, vals.shape[1] // lists, k, ptr(ov), ptr(ol),
+                                     stream_handle(stream)))
+    return ov, ol
+
+
+def scale_rows(vals: torch.Tensor, scaleA: torch.Tensor) -> torch.Tensor:
+    """Apply per-row scales after a merge (empty slots stay -inf).  Scaled
+    scores rank by the value before the row scale -- a shared positive
+    factor can round two different values to one -- so a sharded search runs
+    its shards with a unit row scale, merges, then scales once; the result
+    equals the single-engine search bit for bit."""
+    return torch.where(torch.isneginf(vals), vals, vals * scaleA[:, None])
+
+
 def gather_shard_topk(vals: torch.Tensor, locs: torch.Tensor, col_lo: int, k: int, group=None):
     """All-gather every rank's local top-k (local 1-based ids shifted by its
-    shard offset) and merge them into the global top-k on every rank."""
+    shard offset) and merge them into the global top-k on every rank: on
+    CUDA tensors with the library's merge kernel, otherwise with torch."""
     g = torch.where(locs > 0, locs + col_lo, locs)
     world = dist.get_world_size(group)
     vs = [torch.empty_like(vals) for _ in range(world)]
     ls = [torch.empty_like(g) for _ in range(world)]
     dist.all_gather(vs, vals.contiguous(), group=group)
     dist.all_gather(ls, g.contiguous(), group=group)
-    return merge_topk(torch.cat(vs, dim=1), torch.cat(ls, dim=1), k)
+    cat_v, cat_l = torch.cat(vs, dim=1), torch.cat(ls, dim=1)
+    if cat_v.is_cuda and world <= 32:
+        return merge_topk_lists(cat_v, cat_l, world, k)
+    return merge_topk(cat_v, cat_l, k)
