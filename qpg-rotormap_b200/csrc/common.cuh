@@ -159,8 +159,17 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
           smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void tmem_wait_ld() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// tcgen05.wait::ld with the loaded registers as operands: nothing that reads
+// them can be scheduled before the wait.
+__device__ __forceinline__ void tmem_wait_ld_tied(float (&v)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]),
+                 "+f"(v[7]), "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]),
+                 "+f"(v[14]), "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]),
+                 "+f"(v[21]), "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]),
+                 "+f"(v[28]), "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
+               :
+               : "memory");
 }
 // 32 lanes x 32 consecutive fp32 columns: thread i gets TMEM lane (base+i).
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {

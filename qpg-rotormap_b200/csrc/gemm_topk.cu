@@ -15,10 +15,10 @@
 //               M=128 N=256 K=32, fp32 accumulators double-buffered in TMEM
 //               (2 x 256 of the 512 columns).
 //   warps 2..5  epilogue: one thread per read row (TMEM lane); tcgen05.ld of
-//               32 columns at a time, score transform (fp16 rounding /
-//               column scale), chunk max vs the row's threshold, and
-//               insertion into a register reservoir of the top KT (score
-//               desc, column asc).
+//               32 columns at a time (the next chunk in flight while one is
+//               scored), score transform (fp16 rounding / column scale),
+//               chunk max vs the row's threshold, and insertion into a
+//               register reservoir of the top KT (score desc, column asc).
 // Work unit = (read tile of 128 rows, column split); each unit streams its
 // split's column tiles and leaves a sorted partial list per row; a second
 // kernel merges the splits.  Every mbarrier wait is bounded; a wait that
@@ -117,6 +117,137 @@ struct Reservoir {
   }
   __device__ __forceinline__ void sort_desc() {}
 };
+
+// Column scales of one 32-column chunk: broadcast loads (every lane of the
+// warp reads the same 128 bytes).  Past the index end they read as 1; those
+// columns are masked to -inf before scoring.
+__device__ __forceinline__ void load_scales(float4 (&s)[8], const float *scaleB, long long c0, long long N,
+                                            bool tail) {
+  if (!tail) {
+    const float4 *p = reinterpret_cast<const float4 *>(scaleB + c0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s[q] = __ldg(p + q);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long long c = c0 + 4 * q;
+      s[q].x = c < N ? __ldg(scaleB + c) : 1.f;
+      s[q].y = c + 1 < N ? __ldg(scaleB + c + 1) : 1.f;
+      s[q].z = c + 2 < N ? __ldg(scaleB + c + 2) : 1.f;
+      s[q].w = c + 3 < N ? __ldg(scaleB + c + 3) : 1.f;
+    }
+  }
+}
+
+__device__ __forceinline__ void apply_scales(float (&v)[32], const float4 (&s)[8]) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    v[4 * q] *= s[q].x;
+    v[4 * q + 1] *= s[q].y;
+    v[4 * q + 2] *= s[q].z;
+    v[4 * q + 3] *= s[q].w;
+  }
+}
+
+// Score one 32-column chunk of this thread's row (columns c0 .. c0+31): the
+// chunk max (a depth-5 tree over 8 partial maxima) against the row's threshold decides whether the
+// chunk goes through the insert path, staged 16 values at a time in `scratch`.
+template <int KT>
+__device__ __forceinline__ void score_chunk(Reservoir<KT> &R, float (&v)[32], long long c0, long long N, bool tail,
+                                            bool f16, float *scratch) {
+  if (tail) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (c0 + j >= N) v[j] = -INFINITY;
+  }
+  float m[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) m[j] = fmaxf(fmaxf(v[j], v[j + 8]), fmaxf(v[j + 16], v[j + 24]));
+#pragma unroll
+  for (int w = 4; w >= 1; w >>= 1)
+#pragma unroll
+    for (int j = 0; j < w; ++j) m[j] = fmaxf(m[j], m[j + w]);
+  float mx = m[0];
+  if (f16) mx = round_f16(mx);
+  if (mx > R.thr) {
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) scratch[j] = v[16 * p + j];
+#pragma unroll 1
+      for (int j = 0; j < 16; ++j) {
+        float x = scratch[j];
+        if (f16) x = round_f16(x);
+        if (x > R.thr) R.insert(x, (int)(c0 + 16 * p + j));
+      }
+    }
+  }
+}
+
+// Drain this warp's CH chunks of one accumulator tile (TMEM address `taddr`
+// = its lane quarter and first chunk; columns c_first .. c_first + 32 CH - 1)
+// into the row's reservoir.  Software-pipelined: the TMEM load and the column
+// scales of chunk i + 1 are in flight while chunk i is scored.  Every load is
+// waited for before returning, so the caller may release the accumulator.
+template <int KT, int CH>
+__device__ __forceinline__ void drain_tile(Reservoir<KT> &R, uint32_t taddr, long long c_first, long long N,
+                                           const float *scaleB, bool scaled, bool f16, float *scratch) {
+  static_assert(CH % 2 == 0, "chunks are drained in pairs");
+  const bool tail = c_first + 32LL * CH > N;
+  float va[32], vb[32];
+  float4 s[8];
+  __syncwarp();
+  tmem_ld32(taddr, va);
+  if (scaled) load_scales(s, scaleB, c_first, N, tail);
+#pragma unroll 1
+  for (int i = 0; i < CH; i += 2) {
+    const long long c0 = c_first + 32LL * i;
+    __syncwarp();
+    tmem_wait_ld_tied(va);
+    if (scaled) apply_scales(va, s);
+    tmem_ld32(taddr + (uint32_t)(i + 1) * 32u, vb);
+    if (scaled) load_scales(s, scaleB, c0 + 32, N, tail);
+    score_chunk(R, va, c0, N, tail, f16, scratch);
+    __syncwarp();
+    tmem_wait_ld_tied(vb);
+    if (scaled) apply_scales(vb, s);
+    if (i + 2 < CH) {
+      tmem_ld32(taddr + (uint32_t)(i + 2) * 32u, va);
+      if (scaled) load_scales(s, scaleB, c0 + 64, N, tail);
+    }
+    score_chunk(R, vb, c0 + 32, N, tail, f16, scratch);
+  }
+}
+
+// The same, one chunk at a time: for the 8-warp form with a 32-entry
+// reservoir, whose 168-register budget has no room for a second chunk.
+template <int KT, int CH>
+__device__ __forceinline__ void drain_tile_serial(Reservoir<KT> &R, uint32_t taddr, long long c_first, long long N,
+                                                  const float *scaleB, bool scaled, bool f16, float *scratch) {
+  const bool tail = c_first + 32LL * CH > N;
+#pragma unroll 1
+  for (int i = 0; i < CH; ++i) {
+    const long long c0 = c_first + 32LL * i;
+    float v[32];
+    float4 s[8];
+    __syncwarp();
+    if (scaled) load_scales(s, scaleB, c0, N, tail);
+    tmem_ld32(taddr + (uint32_t)i * 32u, v);
+    tmem_wait_ld_tied(v);
+    if (scaled) apply_scales(v, s);
+    score_chunk(R, v, c0, N, tail, f16, scratch);
+  }
+}
+
+template <int KT, int H>
+__device__ __forceinline__ void drain_acc(Reservoir<KT> &R, uint32_t taddr, long long c_first, long long N,
+                                      const float *scaleB, bool scaled, bool f16, float *scratch) {
+  constexpr int CH = BN / 32 / H;
+  if constexpr (H == 1 || KT < 32)
+    drain_tile<KT, CH>(R, taddr, c_first, N, scaleB, scaled, f16, scratch);
+  else
+    drain_tile_serial<KT, CH>(R, taddr, c_first, N, scaleB, scaled, f16, scratch);
+}
 
 template <int KT, int H>
 __global__ void __launch_bounds__(epi_threads(H), 1)
@@ -294,57 +425,8 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
           break;
         }
         tc_fence_after();
-        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
-        const long long colbase = (long long)t * BN;
-        const bool tail = colbase + BN > g.N;
-#pragma unroll 1
-        for (int ch = half * CH; ch < (half + 1) * CH; ++ch) {
-          float v[32];
-          __syncwarp();
-          tmem_ld32(taddr + ch * 32, v);
-          tmem_wait_ld();
-          const long long c0 = colbase + ch * 32;
-          if (scaled) {
-            if (!tail) {
-              const float4 *sb = reinterpret_cast<const float4 *>(g.scaleB + c0);
-#pragma unroll
-              for (int q = 0; q < 8; ++q) {
-                float4 s4 = __ldg(sb + q);
-                v[4 * q] *= s4.x;
-                v[4 * q + 1] *= s4.y;
-                v[4 * q + 2] *= s4.z;
-                v[4 * q + 3] *= s4.w;
-              }
-            } else {
-#pragma unroll
-              for (int j = 0; j < 32; ++j) v[j] = (c0 + j < g.N) ? v[j] * __ldg(g.scaleB + c0 + j) : v[j];
-            }
-          }
-          if (tail) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (c0 + j >= g.N) v[j] = -INFINITY;
-          }
-          float mx = v[0];
-#pragma unroll
-          for (int j = 1; j < 32; ++j) mx = fmaxf(mx, v[j]);
-          if (f16) mx = round_f16(mx);
-          if (mx > R.thr) {
-            // rare path: stage the chunk (16 values at a time) and insert its
-            // survivors one by one
-#pragma unroll
-            for (int p = 0; p < 2; ++p) {
-#pragma unroll
-              for (int j = 0; j < 16; ++j) scratch[j] = v[16 * p + j];
-#pragma unroll 1
-              for (int j = 0; j < 16; ++j) {
-                float x = scratch[j];
-                if (f16) x = round_f16(x);
-                if (x > R.thr) R.insert(x, (int)(c0 + 16 * p + j));
-              }
-            }
-          }
-        }
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + half * CH * 32);
+        drain_acc<KT, H>(R, taddr, (long long)t * BN + half * CH * 32, g.N, g.scaleB, scaled, f16, scratch);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[acc]);
@@ -571,55 +653,8 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
           break;
         }
         tc_fence_after();
-        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
-        const long long colbase = (long long)t * BN;
-        const bool tail = colbase + BN > g.N;
-#pragma unroll 1
-        for (int ch = half * CH; ch < (half + 1) * CH; ++ch) {
-          float v[32];
-          __syncwarp();
-          tmem_ld32(taddr + ch * 32, v);
-          tmem_wait_ld();
-          const long long c0 = colbase + ch * 32;
-          if (scaled) {
-            if (!tail) {
-              const float4 *sb = reinterpret_cast<const float4 *>(g.scaleB + c0);
-#pragma unroll
-              for (int q = 0; q < 8; ++q) {
-                float4 s4 = __ldg(sb + q);
-                v[4 * q] *= s4.x;
-                v[4 * q + 1] *= s4.y;
-                v[4 * q + 2] *= s4.z;
-                v[4 * q + 3] *= s4.w;
-              }
-            } else {
-#pragma unroll
-              for (int j = 0; j < 32; ++j) v[j] = (c0 + j < g.N) ? v[j] * __ldg(g.scaleB + c0 + j) : v[j];
-            }
-          }
-          if (tail) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (c0 + j >= g.N) v[j] = -INFINITY;
-          }
-          float mx = v[0];
-#pragma unroll
-          for (int j = 1; j < 32; ++j) mx = fmaxf(mx, v[j]);
-          if (f16) mx = round_f16(mx);
-          if (mx > R.thr) {
-#pragma unroll
-            for (int p = 0; p < 2; ++p) {
-#pragma unroll
-              for (int j = 0; j < 16; ++j) scratch[j] = v[16 * p + j];
-#pragma unroll 1
-              for (int j = 0; j < 16; ++j) {
-                float x = scratch[j];
-                if (f16) x = round_f16(x);
-                if (x > R.thr) R.insert(x, (int)(c0 + 16 * p + j));
-              }
-            }
-          }
-        }
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + half * CH * 32);
+        drain_acc<KT, H>(R, taddr, (long long)t * BN + half * CH * 32, g.N, g.scaleB, scaled, f16, scratch);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive_cluster(mapa_shared(smem_u32(&acc_empty[acc]), 0));
@@ -752,7 +787,7 @@ static int get_encode_fn(EncodeTiledFn *fn) {
 // 2-D uint8 tensor of `rows` x `cols` bytes (row stride = cols), box
 // `box_rows` x 128 bytes, 128-byte swizzle, zero fill outside.
 static int make_map(CUtensorMap *map, const void *base, long long rows, int cols, int box_rows) {
-  EncodeTiledFn fn;
+  EncodeTiledFn fn = nullptr;
   int rc = get_encode_fn(&fn);
   if (rc) return rc;
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
