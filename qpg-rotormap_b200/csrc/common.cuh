@@ -96,16 +96,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: spins on the phase with the given parity; gives up after
-// `limit` clock cycles (returns false).  `abort` (shared flag) lets a role
-// that already gave up release every other waiter quickly.
+// try_wait with a suspend-time hint: a thread whose phase is not complete is
+// suspended until it completes or about `ns` nanoseconds pass, instead of
+// returning after the hardware's default interval.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on the phase with the given parity; gives up after `limit`
+// clock cycles (returns false).  Between checks the thread sleeps in
+// try_wait (up to 0.1 ms), so waiting warps issue almost nothing.  `abort`
+// (shared flag) lets a role that already gave up release every other waiter.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
                                                   volatile int *abort,
                                                   long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   long long t0 = clock64();
   while (true) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_sleep(bar, parity, 100000u)) return true;
     if (*abort) return false;
     if (clock64() - t0 > limit) return false;
   }

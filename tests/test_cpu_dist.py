@@ -1,5 +1,6 @@
 """The N > 1 paths on CPU with gloo, world size 2: max-over-ranks timing and
-the column-sharded top-k gather/merge (equal to the unsharded top-k)."""
+the column-sharded top-k gather/merge (equal to the unsharded top-k, with
+fp16-rounded and with scaled scores)."""
 import os
 import socket
 
@@ -18,6 +19,11 @@ def _free_port():
     p = s.getsockname()[1]
     s.close()
     return p
+
+
+def _scales(nb, N):
+    rng = np.random.default_rng(3)
+    return rng.uniform(0.5, 2.0, nb).astype(np.float32), rng.uniform(0.5, 2.0, N).astype(np.float32)
 
 
 def _worker(rank, world, port, q):
@@ -40,7 +46,12 @@ def _worker(rank, world, port, q):
         lo, hi = rdist.shard_bounds(B.shape[0], world, rank)
         v, l = orc.topk_e4m3(A, B[lo:hi], 20, 0)
         gv, gl = rdist.gather_shard_topk(torch.from_numpy(v), torch.from_numpy(l), lo, 20)
-        q.put((rank, t, gv.numpy(), gl.numpy()))
+        # scaled scores: shards rank with a unit row scale, the row scale comes after the merge
+        sa, sb = _scales(A.shape[0], B.shape[0])
+        v, l = orc.topk_e4m3(A, B[lo:hi], 20, 2, np.ones(A.shape[0], np.float32), sb[lo:hi])
+        sv, sl = rdist.gather_shard_topk(torch.from_numpy(v), torch.from_numpy(l), lo, 20)
+        sv = rdist.scale_rows(sv, torch.from_numpy(sa))
+        q.put((rank, t, gv.numpy(), gl.numpy(), sv.numpy(), sl.numpy()))
     finally:
         dist.barrier()
         dist.destroy_process_group()
@@ -62,9 +73,12 @@ def test_two_rank_gloo_timing_and_sharded_topk():
     A = E[rng.integers(0, 7, (50, 64))]
     B = E[rng.integers(0, 7, (3001, 64))]
     rv, rl = orc.topk_e4m3(A, B, 20, 0)
-    for rank, t, gv, gl in res:
+    sa, sb = _scales(A.shape[0], B.shape[0])
+    qv, ql = orc.topk_e4m3(A, B, 20, 2, sa, sb)
+    for rank, t, gv, gl, sv, sl in res:
         assert t == [2.0, 5.0]
         assert np.array_equal(gv, rv) and np.array_equal(gl, rl)
+        assert np.array_equal(sv, qv) and np.array_equal(sl, ql)
 
 
 def test_shard_bounds_cover_every_column():
