@@ -67,6 +67,12 @@ int r2m_device_check(void);
  * check on the current device.  No reference counterpart: the reference's
  * kernels have no bounded waits. */
 int r2m_check_device_error(r2m_stream_t stream);
+/* Self-check of that mechanism: one CTA waits, with the kernels' bounded
+ * wait and a limit of `limit_cycles` SM clocks (<= 4e9), on an mbarrier that
+ * nothing arrives on (arrive = 0: the wait gives up and the next
+ * r2m_check_device_error reports R2M_ETIMEOUT) or that it completed itself
+ * (arrive = 1: no error).  Stream-ordered; touches no caller memory. */
+int r2m_selftest_bounded_wait(int64_t limit_cycles, int arrive, r2m_stream_t stream);
 
 /* ---------------------------------------------------------------- encode */
 

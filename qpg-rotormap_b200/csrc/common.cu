@@ -108,9 +108,40 @@ int check_device_error(cudaStream_t stream, const char *what) {
   return R2M_OK;
 }
 
+// One CTA waits, through the same bounded wait the pipelined kernels use, on
+// an mbarrier that nothing arrives on (or, with `arrive`, that its own thread
+// completed first); a wait that gives up records its code in the device
+// error word like a kernel's would.
+__global__ void k_selftest_wait(long long limit, int arrive, uint32_t *err) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (arrive) mbar_arrive(&bar);
+    if (!mbar_wait_bounded(&bar, 0, &abort_flag, limit)) atomicExch(err, kErrTimeoutSelfTest);
+  }
+  __syncthreads();
+}
+
 }  // namespace r2m
 
 extern "C" {
+
+int r2m_selftest_bounded_wait(int64_t limit_cycles, int arrive, r2m_stream_t stream) {
+  if (limit_cycles < 0 || limit_cycles > (int64_t)4000000000LL)
+    return r2m::fail(R2M_EINVAL, "limit_cycles must be in 0..4e9");
+  uint32_t *w = nullptr;
+  int rc = r2m::device_error_word(&w);
+  if (rc) return rc;
+  r2m::k_selftest_wait<<<1, 32, 0, r2m::as_stream(stream)>>>((long long)limit_cycles, arrive ? 1 : 0, w);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
 
 const char *r2m_last_error(void) { return r2m::g_last_error.c_str(); }
 

@@ -58,6 +58,7 @@ enum : uint32_t {
   kErrTimeoutAccFull = 3,
   kErrTimeoutAccEmpty = 4,
   kErrTimeoutDrain = 5,
+  kErrTimeoutSelfTest = 6,
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {

@@ -42,6 +42,7 @@ SIGNATURES = [
     ("r2m_version", I, []),
     ("r2m_device_check", I, []),
     ("r2m_check_device_error", I, [P]),
+    ("r2m_selftest_bounded_wait", I, [I64, I, P]),
     ("r2m_encode_frag_real_batch", I, [P, I, P, P, P, I64, I, I, I, I, I, P]),
     ("r2m_revcomp_frag_words", I, [P, P, I, I64, P]),
     ("r2m_encode_ref_windows", I, [P, I, P, P, P, P, I64, I64, I, I, I, I, I, P]),
