@@ -135,7 +135,11 @@ typedef struct {
                       1 single-CTA, 2 CTA-pair;
                       reserved[2]: epilogue form of either kernel, 0 auto
                       (8 warps for work units of at most 8192 column tiles,
-                      else 4), 1 four warps, 2 eight warps (k <= 32) */
+                      else 4), 1 four warps, 2 eight warps (k <= 32);
+                      reserved[3]: pacing of the CTA-pair kernel, 0 default
+                      (a pair naps while it is more than 16 column tiles
+                      ahead of the slowest pair, so the pairs share index
+                      tiles through L2), > 0 that window in tiles, < 0 off */
 } r2m_tuning;
 
 /* Replaces TopKEngine(B; k, w, rows_cap, segs, engine, cout)

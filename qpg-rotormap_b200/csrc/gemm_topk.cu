@@ -70,6 +70,8 @@ struct GemmArgs {
   float *part_vals;
   int *part_cols;
   uint32_t *err;
+  long long *pace;  // CTA-pair kernel: per-pair progress (null = no pacing)
+  int pace_window;  // column tiles a pair may run ahead of the slowest one
 };
 
 __device__ __forceinline__ int split_lo(int s, int n_tiles, int splits) {
@@ -471,6 +473,39 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
 // multicast is used anywhere.
 constexpr int STAGES2 = 6;
 constexpr int HALF_TILE = 128 * BK;  // 16 KiB
+
+// Pair pacing.  Every pair streams the index in column order, and the pairs
+// of one wave (units p, p + npairs, ... run side by side) read the same index
+// tiles, so a tile comes from DRAM once and from L2 for the other pairs --
+// while the pairs stay within an L2's worth of tiles of each other.  Left
+// alone they drift apart over a long unit, and then every pair streams the
+// index from DRAM itself.  So each pair's producer publishes its position
+// (column tiles issued since the launch; -1 = not started, LLONG_MAX = done)
+// every PACE_EVERY tiles and, while it is more than `window` tiles ahead of
+// the slowest started pair, sleeps -- for at most PACE_CHECKS short naps.
+// Pacing only ever delays a pair a little: it never waits for a pair that is
+// not running, and it cannot stall the launch.
+// Same-box sweep on 65,536 reads x 16.8M columns (mean of two launches):
+// no pacing 1,761 ms; window 16 checked every 16 tiles 1,667 ms; windows of
+// 32 / 64 / 128 tiles 1,693 / 1,717 / 1,732 ms; tighter windows or checks
+// every 8 or 4 tiles 1,698-1,837 ms (the naps and reads start to cost).
+constexpr int PACE_EVERY = 16;
+constexpr int PACE_CHECKS = 16;
+constexpr int PACE_WINDOW = 16;  // tiles of 256 columns: 8 MiB of a 2048-byte index
+
+__device__ __forceinline__ void pace_pair(long long *pace, int pair, int npairs, long long pos, int window) {
+  volatile long long *p = pace;
+  p[pair] = pos;
+  for (int it = 0; it < PACE_CHECKS; ++it) {
+    long long mn = LLONG_MAX;
+    for (int q = 0; q < npairs; ++q) {
+      const long long v = p[q];
+      if (v >= 0 && v < mn) mn = v;
+    }
+    if (pos - mn <= window) return;
+    __nanosleep(1000);
+  }
+}
 // CTA-pair kernel: TMA warp, MMA warp and 4 * H epilogue warps (epilogue
 // forms above).
 template <int KT, int H>
@@ -530,11 +565,14 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
       int stage = 0;
       uint32_t phase = 0;
       long long issued = 0;
+      long long pos = 0;  // column tiles this pair issued in earlier units
+      const bool pacing = leader && g.pace != nullptr;
       bool ok = true;
       for (int u = pair; ok && u < num_units; u += npairs) {
         const int mt = u % g.num_m_tiles, sp = u / g.num_m_tiles;
         const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
         for (int t = t0; ok && t < t1; ++t) {
+          if (pacing && (t - t0) % PACE_EVERY == 0) pace_pair(g.pace, pair, npairs, pos + (t - t0), g.pace_window);
           for (int kb = 0; kb < g.num_kb; ++kb) {
             if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, abort_flag, WAIT_LIMIT)) {
               if (!*abort_flag) atomicExch(g.err, kErrTimeoutEmpty);
@@ -553,7 +591,9 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
             }
           }
         }
+        pos += t1 - t0;
       }
+      if (pacing) reinterpret_cast<volatile long long *>(g.pace)[pair] = LLONG_MAX;  // holds no one back
       if (!ok && leader) {
         int nlast = issued < STAGES2 ? (int)issued : STAGES2;
         for (int j = 1; j <= nlast; ++j) {
@@ -891,6 +931,16 @@ static int kernel_kind(int mode, int nb) {
   return nb > BM ? 2 : 1;
 }
 
+// Progress slots for pair pacing (one per CTA pair of a launch).
+constexpr int kPaceSlots = 1024;
+
+// Pacing window of the CTA-pair kernel from tuning.reserved[3]: 0 = the
+// default, > 0 = that many column tiles, < 0 = no pacing.
+static int pace_window_for(const r2m_tuning *tune) {
+  const int r = tune ? tune->reserved[3] : 0;
+  return r < 0 ? 0 : r == 0 ? PACE_WINDOW : r;
+}
+
 // Split lists the workspace must hold for any batch height up to rows_cap.
 static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int mode, int KT) {
   size_t lists = 0;
@@ -933,6 +983,8 @@ struct r2m_engine {
   int *part_cols;
   size_t part_lists;  // capacity in lists (rows x splits)
   uint32_t *err;
+  long long *pace;    // per-pair progress of the CTA-pair kernel (kPaceSlots)
+  int pace_window;    // 0 = no pacing
   bool timing;        // record events around the two kernels of each call
   cudaEvent_t ev[3];
   int last_splits;
@@ -972,6 +1024,7 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   if (e->mode < 0 || e->mode > 2) e->mode = 0;
   e->epi = tune ? tune->reserved[2] : 0;
   if (e->epi < 0 || e->epi > 2) e->epi = 0;
+  e->pace_window = pace_window_for(tune);
   e->last_splits = 0;
   if (e->timing) {
     for (int i = 0; i < 3; ++i) {
@@ -994,8 +1047,10 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   e->part_lists = lists;
   cudaError_t ce = cudaMalloc(&e->part_vals, lists * e->KT * sizeof(float));
   if (ce == cudaSuccess) ce = cudaMalloc(&e->part_cols, lists * e->KT * sizeof(int));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->pace, kPaceSlots * sizeof(long long));
   if (ce != cudaSuccess) {
     cudaFree(e->part_vals);
+    cudaFree(e->part_cols);
     delete e;
     return fail(R2M_ENOMEM, "engine workspace allocation failed");
   }
@@ -1003,6 +1058,7 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   if (rc) {
     cudaFree(e->part_vals);
     cudaFree(e->part_cols);
+    cudaFree(e->pace);
     delete e;
     return rc;
   }
@@ -1014,6 +1070,7 @@ extern "C" int r2m_engine_destroy(r2m_engine *eng) {
   if (!eng) return R2M_OK;
   cudaFree(eng->part_vals);
   cudaFree(eng->part_cols);
+  cudaFree(eng->pace);
   if (eng->timing)
     for (int i = 0; i < 3; ++i) cudaEventDestroy(eng->ev[i]);
   delete eng;
@@ -1046,6 +1103,7 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   eng->forced_splits = forced;
   eng->mode = mode;
   eng->epi = (tune->reserved[2] >= 0 && tune->reserved[2] <= 2) ? tune->reserved[2] : 0;
+  eng->pace_window = pace_window_for(tune);
   return R2M_OK;
 }
 
@@ -1115,6 +1173,14 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   long long units = (long long)g.num_m_tiles * g.splits;
   int ctas = (int)(units < ctas_eff ? units : ctas_eff);
   eng->last_splits = g.splits;
+  g.pace = nullptr;
+  g.pace_window = 0;
+  if (kind == 2 && eng->pace_window > 0 && ctas > 1 && ctas <= kPaceSlots) {
+    // every pair starts as "not started" (-1)
+    R2M_CUDA(cudaMemsetAsync(eng->pace, 0xFF, (size_t)ctas * sizeof(long long), st));
+    g.pace = eng->pace;
+    g.pace_window = eng->pace_window;
+  }
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[0], st));
   if (kind == 2) {
     if (halves == 2) {
@@ -1281,6 +1347,8 @@ extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_sc
   g.part_vals = reinterpret_cast<float *>(scratch);
   g.part_cols = reinterpret_cast<int *>(scratch + (size_t)splits * g.mpad * KT * sizeof(float));
   g.err = err;
+  g.pace = nullptr;  // the single-CTA kernel does not pace
+  g.pace_window = 0;
   // the error word must start at zero; the partial lists are fully
   // rewritten by the kernel before the merge reads them
   R2M_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
