@@ -41,9 +41,10 @@ Q = 65_536
 N_COLS = 16_777_216
 TOPK = 20
 # DRAM bytes (read + write) of one fused launch at the default workload
-# (65,536 reads x 16,777,216 columns), from a one-pass ncu capture of the
-# bench command (profiles/k_gemm_topk2_65536x16777216_dram.md)
-FUSED_DRAM_BYTES = 281_160_000_000 + 169_600_000
+# (65,536 reads x 16,777,216 columns): the mean over the 9 launches of a
+# one-pass ncu capture of the bench command
+# (profiles/k_gemm_topk2_65536x16777216_dram.md)
+FUSED_DRAM_BYTES = 138_477_900_000 + 90_320_000
 ERR = 0.05
 GENOME_SEED, READ_SEED = 7, 11
 METRIC = "reads/s on 1 B200 at top-20 recall = ref, serving vs plain; p50/p99 latency"
@@ -789,7 +790,8 @@ def main():
                          "traffic_algorithmic": nq * re.rdim + N * re.rdim,
                          "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
                                          "workload (ncu, 1 pass; profiles/k_gemm_topk2_65536x16777216_dram.md): "
-                                         "the index streamed ~8x by CTA pairs that drift apart, at ~2.4% of HBM",
+                                         "the index read ~4x (once per wave of paced CTA pairs, each index "
+                                         "tile shared through L2 within a wave), ~1.2% of HBM",
                          "kernel": ("k_gemm_topk2 (CTA-pair tcgen05 fp8 GEMM + fused top-20)" if nq > 128 else
                                     "k_gemm_topk (single-CTA tcgen05 fp8 GEMM + fused top-20)"),
                          "peak_basis": f"dense fp8 = 2 x {basis} sustained bf16 "
