@@ -179,9 +179,10 @@ int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A,
                         int32_t *d_locs, r2m_stream_t stream);
 
 /* Allocation-free variant of r2m_batch_gemm_topk for callers that cannot
- * allocate device memory when they search: a thread capturing a CUDA graph,
- * a serving loop where cudaMalloc would synchronize the device, or a host
- * whose memory pool already owns the free device memory.  No counterpart in
+ * allocate device memory when they search: a serving loop where cudaMalloc
+ * would synchronize the device and stall its other streams, or a host whose
+ * memory pool (CUDA.jl's, PyTorch's caching allocator) already owns the free
+ * device memory, so a side allocation can fail.  No counterpart in
  * the reference.  Takes the engine's arguments directly (B, scaleB, rdim, N,
  * k, score_mode as r2m_engine_create; A, scaleA, nb, outputs as
  * r2m_batch_gemm_topk) and calls no cudaMalloc/cudaFree: the split scratch

@@ -1245,14 +1245,16 @@ extern "C" int r2m_engine_kernel_ms(r2m_engine *eng, float *gemm_ms, float *merg
 // Allocation-free search.
 //
 // Some callers cannot allocate device memory at the point where they map a
-// batch: a thread that is capturing a CUDA graph, a serving loop where a
-// cudaMalloc would synchronize the device and stall other streams, or a host
-// whose memory pool (CUDA.jl's, PyTorch's caching allocator) already owns the
-// free device memory, so a side allocation can fail.  This entry point needs
-// no engine: the per-split partial top-k lists live in the file-scope array
-// below, whose device address is looked up once per device with
-// cudaGetSymbolAddress.  Every GPU that loads this library holds the array
-// (kNoAllocScratchBytes) until the process exits.
+// batch: a serving loop where a cudaMalloc would synchronize the device and
+// stall other streams, or a host whose memory pool (CUDA.jl's, PyTorch's
+// caching allocator) already owns the free device memory, so a side
+// allocation can fail.  This entry point needs no engine: the per-split
+// partial top-k lists live in the file-scope array below, whose device
+// address is looked up with cudaGetSymbolAddress by the first call on each
+// device (so that first call should come before any stream capture).  Every
+// GPU that loads this library holds the array (kNoAllocScratchBytes) until
+// the process exits; all calls share it, so calls that overlap on the GPU
+// race.
 namespace r2m {
 
 constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB

@@ -1,8 +1,8 @@
 """The allocation-free search entry point (r2m_batch_gemm_topk_noalloc).
 
 It serves callers that cannot allocate device memory while they map reads
-(graph-capturing threads, latency-bound serving loops, hosts whose memory
-pool owns the device).  Its results must equal the engine path's
+(latency-bound serving loops, where a cudaMalloc would synchronize the
+device, and hosts whose memory pool owns the device memory).  Its results must equal the engine path's
 (r2m_batch_gemm_topk) on the same inputs, call after call: the shared scratch
 keeps the previous call's contents, which must not leak into the next.
 This file is collected last so a failure here comes after every other test.
