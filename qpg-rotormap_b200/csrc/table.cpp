@@ -11,13 +11,19 @@
 // digits come from std::to_chars, which returns the shortest string that
 // reads back to the same float (ties resolved to the closest).
 //
-// Rows are split into blocks formatted by separate threads and concatenated
-// in order.
+// Rows are split into blocks; each thread writes its block's lines through a
+// raw pointer into its own buffer (sized by an upper bound per line), then
+// the threads copy their blocks side by side into the output buffer.  The
+// buffers come from a small pool that keeps them mapped between calls, so a
+// batch does not pay page faults on 100 MB of fresh memory every time.
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <charconv>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -28,8 +34,56 @@ namespace r2m {
 int fail(int code, const std::string &msg);
 }  // namespace r2m
 
+namespace {
+
+struct Buf {
+  char *p = nullptr;
+  size_t cap = 0;
+};
+
+// Free buffers kept for reuse: at most kPoolBufs of them and kPoolBytes in all.
+constexpr size_t kPoolBufs = 64;
+constexpr size_t kPoolBytes = size_t(1) << 30;
+std::mutex g_pool_mu;
+std::vector<Buf> g_pool;
+
+// A buffer of at least `need` bytes: the smallest pooled one that fits, else
+// a new one (nullptr p on allocation failure).
+Buf take_buf(size_t need) {
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    size_t best = g_pool.size();
+    for (size_t i = 0; i < g_pool.size(); ++i)
+      if (g_pool[i].cap >= need && (best == g_pool.size() || g_pool[i].cap < g_pool[best].cap)) best = i;
+    if (best < g_pool.size()) {
+      Buf b = g_pool[best];
+      g_pool.erase(g_pool.begin() + (long)best);
+      return b;
+    }
+  }
+  Buf b;
+  b.p = static_cast<char *>(malloc(need ? need : 1));
+  b.cap = b.p ? need : 0;
+  return b;
+}
+
+void give_buf(Buf b) {
+  if (!b.p) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  size_t tot = b.cap;
+  for (auto &x : g_pool) tot += x.cap;
+  if (g_pool.size() < kPoolBufs && tot <= kPoolBytes) {
+    g_pool.push_back(b);
+    return;
+  }
+  free(b.p);
+}
+
+}  // namespace
+
 struct r2m_text {
-  std::string s;
+  Buf b;
+  size_t n = 0;
 };
 
 namespace {
@@ -143,20 +197,26 @@ extern "C" int r2m_format_table(const float *vals, const int32_t *locs, int64_t 
   if (!split_lines(rec_names, rec_names_len, -1, rn) || rn.empty())
     return r2m::fail(R2M_EINVAL, "rec_names must hold '\\n'-terminated record names");
   const int64_t nrec = (int64_t)rn.size();
-  for (int64_t i = 0; i < nb * (int64_t)k; ++i) {
-    const int64_t c = (int64_t)locs[i] - 1;
-    if (c < 0 || c >= ncols) return r2m::fail(R2M_EINVAL, "location out of range (1-based, 1..N)");
-    if (col_rec[c] < 0 || col_rec[c] >= nrec) return r2m::fail(R2M_EINVAL, "column record id out of range");
-  }
+  size_t max_rec = 0;
+  for (auto &x : rn) max_rec = std::max(max_rec, x.second);
   if (nthreads < 1) nthreads = 1;
   const int64_t nblk = nb < 2048 ? 1 : std::min<int64_t>(nthreads, (nb + 1023) / 1024);
-  std::vector<std::string> part((size_t)nblk);
-  auto work = [&](int64_t b) {
+  // per line: header + " + " + score (<= 32) + ' ' + start (<= 20) + ' ' + record name + '\n'
+  const size_t line_extra = 3 + 32 + 1 + 20 + 1 + max_rec + 1;
+  std::vector<Buf> part((size_t)nblk);
+  std::vector<size_t> used((size_t)nblk, 0);
+  std::atomic<int> bad{0};  // 1 = location out of range, 2 = record id out of range, 3 = no memory
+  auto format = [&](int64_t b) {
     const int64_t r0 = nb * b / nblk, r1 = nb * (b + 1) / nblk;
-    std::string &s = part[(size_t)b];
-    s.reserve((size_t)(r1 - r0) * k * 64);
-    char num[48];
-    for (int64_t r = r0; r < r1; ++r) {
+    size_t bound = 0;
+    for (int64_t r = r0; r < r1; ++r) bound += (size_t)k * (hd[(size_t)r].second + line_extra);
+    Buf buf = take_buf(bound);
+    if (!buf.p) {
+      bad = 3;
+      return;
+    }
+    char *w = buf.p;
+    for (int64_t r = r0; r < r1 && !bad.load(std::memory_order_relaxed); ++r) {
       const char *h = heads + hd[(size_t)r].first;
       size_t hl = hd[(size_t)r].second;
       if (hl && h[0] == '>') {
@@ -165,38 +225,75 @@ extern "C" int r2m_format_table(const float *vals, const int32_t *locs, int64_t 
       }
       for (int j = 0; j < k; ++j) {
         const int64_t c = (int64_t)locs[r * k + j] - 1;
-        s.append(h, hl);
-        s.append(strand[c] == 0 ? " + " : " - ");
-        s.append(num, (size_t)julia_f32(vals[r * k + j], num));
-        s.push_back(' ');
-        auto q = std::to_chars(num, num + sizeof(num), starts[c] - 1);
-        s.append(num, (size_t)(q.ptr - num));
-        s.push_back(' ');
-        const auto &nm = rn[(size_t)col_rec[c]];
-        s.append(rec_names + nm.first, nm.second);
-        s.push_back('\n');
+        if (c < 0 || c >= ncols) {
+          bad = 1;
+          break;
+        }
+        const int32_t rec = col_rec[c];
+        if (rec < 0 || rec >= nrec) {
+          bad = 2;
+          break;
+        }
+        memcpy(w, h, hl);
+        w += hl;
+        w[0] = ' ';
+        w[1] = strand[c] == 0 ? '+' : '-';
+        w[2] = ' ';
+        w += 3;
+        w += julia_f32(vals[r * k + j], w);
+        *w++ = ' ';
+        w = std::to_chars(w, w + 20, starts[c] - 1).ptr;
+        *w++ = ' ';
+        const auto &nm = rn[(size_t)rec];
+        memcpy(w, rec_names + nm.first, nm.second);
+        w += nm.second;
+        *w++ = '\n';
       }
     }
+    part[(size_t)b] = buf;
+    used[(size_t)b] = (size_t)(w - buf.p);
   };
-  if (nblk == 1) {
-    work(0);
-  } else {
+  auto run = [&](auto &&fn) {
+    if (nblk == 1) {
+      fn(0);
+      return;
+    }
     std::vector<std::thread> th;
-    for (int64_t b = 0; b < nblk; ++b) th.emplace_back(work, b);
+    for (int64_t b = 0; b < nblk; ++b) th.emplace_back(fn, b);
     for (auto &t : th) t.join();
+  };
+  run(format);
+  if (bad) {
+    for (auto &b : part) give_buf(b);
+    if (bad == 1) return r2m::fail(R2M_EINVAL, "location out of range (1-based, 1..N)");
+    if (bad == 2) return r2m::fail(R2M_EINVAL, "column record id out of range");
+    return r2m::fail(R2M_ENOMEM, "table buffer allocation failed");
   }
+  std::vector<size_t> off((size_t)nblk + 1, 0);
+  for (int64_t b = 0; b < nblk; ++b) off[(size_t)b + 1] = off[(size_t)b] + used[(size_t)b];
   r2m_text *t = new r2m_text();
-  size_t tot = 0;
-  for (auto &p : part) tot += p.size();
-  t->s.reserve(tot);
-  for (auto &p : part) t->s.append(p);
+  t->b = take_buf(off.back());
+  t->n = off.back();
+  if (!t->b.p) {
+    for (auto &b : part) give_buf(b);
+    delete t;
+    return r2m::fail(R2M_ENOMEM, "table buffer allocation failed");
+  }
+  run([&](int64_t b) {
+    memcpy(t->b.p + off[(size_t)b], part[(size_t)b].p, used[(size_t)b]);
+    give_buf(part[(size_t)b]);
+  });
   *out = t;
   return R2M_OK;
 }
 
 extern "C" const char *r2m_text_data(const r2m_text *t, size_t *len) {
-  if (len) *len = t ? t->s.size() : 0;
-  return t ? t->s.data() : nullptr;
+  if (len) *len = t ? t->n : 0;
+  return t ? t->b.p : nullptr;
 }
 
-extern "C" void r2m_text_free(r2m_text *t) { delete t; }
+extern "C" void r2m_text_free(r2m_text *t) {
+  if (!t) return;
+  give_buf(t->b);
+  delete t;
+}

@@ -94,13 +94,16 @@ def write_table(io, vals, locs, heads, idx: Index, recname=None, nthreads: int |
     try:
         n = ctypes.c_size_t()
         p = L.r2m_text_data(h, ctypes.byref(n))
-        data = ctypes.string_at(p, n.value)
+        if n.value:
+            # written straight from the library's buffer (no bytes copy)
+            view = memoryview((ctypes.c_char * n.value).from_address(p)).cast("B")
+            if isinstance(io, _io.TextIOBase):
+                io.write(bytes(view).decode("latin-1"))
+            else:
+                io.write(view)
+            view.release()
     finally:
         L.r2m_text_free(h)
-    if isinstance(io, _io.TextIOBase):
-        io.write(data.decode("latin-1"))
-    else:
-        io.write(data)
     return nb * k
 
 
