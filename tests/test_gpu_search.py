@@ -195,3 +195,35 @@ def test_pair_kernel_forced_epilogue_forms(k, kernel):
     with pytest.raises(ValueError):
         eng.set_tuning(epilogue="6")
     eng.close()
+
+
+@pytest.mark.parametrize("epilogue", ["4", "8"])
+@pytest.mark.parametrize("score", ["f16", "scaled"])
+def test_pair_pacing_changes_only_the_schedule(epilogue, score):
+    """Pair pacing (tuning reserved[3]) delays pairs but computes nothing
+    differently: unpaced, the default window, the tightest window (1 tile)
+    and a window wider than the index give identical values, locations and
+    tie order, search after search, equal to the oracle."""
+    rng = np.random.default_rng(41)
+    nb, N, rdim = 600, 200_001, 128  # 3 pair read tiles x 782 column tiles
+    A8, _ = int_e4m3(rng, (nb, rdim), -1, 1)
+    B8, _ = int_e4m3(rng, (N, rdim), -1, 1)
+    sa = rng.uniform(0.5, 2.0, nb).astype(np.float32) if score == "scaled" else None
+    sb = rng.uniform(0.5, 2.0, N).astype(np.float32) if score == "scaled" else None
+    B = torch.from_numpy(B8).cuda()
+    A = torch.from_numpy(A8).cuda()
+    sbt = torch.from_numpy(sb).cuda() if sb is not None else None
+    sat = torch.from_numpy(sa).cuda() if sa is not None else None
+    eng = rm.TopKEngine(B, k=20, rows_cap=nb, score=score, scaleB=sbt, kernel="2sm", epilogue=epilogue)
+    outs = []
+    for pace in (-1, 0, 1, 1 << 20, 0):
+        eng.set_tuning(kernel="2sm", epilogue=epilogue, pace=pace)
+        v, l = eng.search(A, nb, sat)
+        torch.cuda.synchronize()
+        outs.append((v.cpu().numpy(), l.cpu().numpy()))
+    from rotormap._lib import check, lib
+    check(lib().r2m_check_device_error(None))
+    eng.close()
+    rv, rl = orc.topk_e4m3(A8, B8, 20, 2 if score == "scaled" else 0, sa, sb)
+    for v, l in outs:
+        assert np.array_equal(v, rv) and np.array_equal(l, rl)
