@@ -333,6 +333,38 @@ def test_native_table_matches_oracle(nb, tmp_path):
         write_table(_io.BytesIO(), vals, bad, heads, idx)
 
 
+def test_native_table_buffers_reused_across_calls():
+    """The writer's buffers are pooled between calls: tables of different
+    sizes and thread counts, one after another (with a rejected call in
+    between), are each exactly the oracle's lines -- nothing left over from
+    an earlier, larger table."""
+    import io as _io
+    from rotormap.mapping import write_table
+
+    class Idx:
+        pass
+    rng = np.random.default_rng(99)
+    N, k = 20_000, 8
+    idx = Idx()
+    idx.strand = rng.integers(0, 2, N).astype(np.uint8)
+    idx.starts = rng.integers(1, 10 ** 6, N).astype(np.int64)
+    idx.col_rec = rng.integers(0, 2, N).astype(np.int32)
+    idx.rec_heads = [">a", ">bb long name"]
+    for nb, nt in ((6000, 8), (3, 1), (4100, 2), (6000, 8), (1, 4), (2500, 3)):
+        vals = rng.uniform(-2, 2, (nb, k)).astype(np.float32)
+        locs = rng.integers(1, N + 1, (nb, k)).astype(np.int32)
+        heads = [f">r{nb}_{i}" + "x" * int(rng.integers(0, 40)) for i in range(nb)]
+        want = orc.table_lines_ref(vals, locs, heads, idx.strand, idx.starts, idx.col_rec, ["a", "bb"])
+        b = _io.BytesIO()
+        write_table(b, vals, locs, heads, idx, nthreads=nt)
+        assert b.getvalue().decode() == want
+        if nb == 4100:
+            bad = locs.copy()
+            bad[-1, -1] = 0
+            with pytest.raises(rm.R2MError):
+                write_table(_io.BytesIO(), vals, bad, heads, idx, nthreads=nt)
+
+
 def test_header_list_behaves_like_a_list():
     hs = [">a one", ">b", "", ">c three words", ">" + "x" * 300]
     blob = ("\n".join(hs) + "\n").encode()
