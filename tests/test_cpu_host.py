@@ -333,6 +333,35 @@ def test_native_table_matches_oracle(nb, tmp_path):
         write_table(_io.BytesIO(), vals, bad, heads, idx)
 
 
+def test_native_table_special_scores():
+    """Scores the float formatter treats specially -- NaN, +-Inf, +-0,
+    subnormals, the decimal/scientific boundaries -- in whole table lines,
+    threaded, byte for byte as the oracle writes them."""
+    import io as _io
+    from rotormap.mapping import write_table
+
+    class Idx:
+        pass
+    special = np.array([np.nan, np.inf, -np.inf, 0.0, -0.0, 1e-45, -1e-45, 1.1754942e-38, 1e-5, 9.999999e-5,
+                        1e-4, 99999.99, 999999.94, 1e6, -1e6, 3.4028235e38, 0.1, -2.5], np.float32)
+    rng = np.random.default_rng(17)
+    nb, k, N = 3000, len(special), 1000
+    idx = Idx()
+    idx.strand = rng.integers(0, 2, N).astype(np.uint8)
+    idx.starts = rng.integers(1, 10 ** 12, N).astype(np.int64)
+    idx.col_rec = np.zeros(N, np.int32)
+    idx.rec_heads = [">only"]
+    vals = np.tile(special, (nb, 1))
+    for r in range(nb):
+        rng.shuffle(vals[r])
+    locs = rng.integers(1, N + 1, (nb, k)).astype(np.int32)
+    heads = [f">q{i}" for i in range(nb)]
+    want = orc.table_lines_ref(vals, locs, heads, idx.strand, idx.starts, idx.col_rec, ["only"])
+    b = _io.BytesIO()
+    write_table(b, vals, locs, heads, idx, nthreads=4)
+    assert b.getvalue().decode() == want
+
+
 def test_native_table_buffers_reused_across_calls():
     """The writer's buffers are pooled between calls: tables of different
     sizes and thread counts, one after another (with a rejected call in
