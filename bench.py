@@ -572,7 +572,11 @@ def map_leg(dev, n_reads: int = 400_000, ncols: int = 1_048_576, seed: int = 91)
         fa = os.path.join(tdir, "reads.fa")
         with open(fa, "wb") as f:
             f.write(raw)
-        rm.run_map(idx, fa, os.path.join(tdir, "warm.maps"), topk=TOPK, batch_size=65_536)
+        warm = os.path.join(tdir, "warm.maps")
+        rm.run_map(idx, fa, warm, topk=TOPK, batch_size=65_536)
+        # each ~540 MB table is deleted before the next run, so the next run
+        # does not write while the kernel still flushes the previous file
+        os.remove(warm)
         for reader in ("device", "host"):
             dst = os.path.join(tdir, f"{reader}.maps")
             torch.cuda.synchronize()
@@ -581,6 +585,7 @@ def map_leg(dev, n_reads: int = 400_000, ncols: int = 1_048_576, seed: int = 91)
             dt = time.perf_counter() - t0
             with open(dst, "rb") as f:
                 lines = sum(1 for _ in f)
+            os.remove(dst)
             out[f"run_map_{reader}_reader"] = {"seconds": dt, "reads_per_s": n / dt, "lines": lines}
     eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=65_536)
     a8, _ = rm.encode_frag_real_batch_alloc(torch.uint8, re, torch.from_numpy(rw[:65_536].view(np.int32)).to(dev))
