@@ -39,8 +39,10 @@ def headline():
     torch.cuda.synchronize()
     check(lib().r2m_check_device_error(None))
     eng.close()
-    yield {"B": idx.embeds8, "sb": sb, "a8": a8, "sa": sa, "v": v.clone(), "l": l.clone(),
-           "starts0": starts0, "col_start": np.asarray(idx.starts), "N": idx.N}
+    h = {"B": idx.embeds8, "sb": sb, "a8": a8, "sa": sa, "v": v.clone(), "l": l.clone(),
+         "starts0": starts0, "col_start": np.asarray(idx.starts), "N": idx.N}
+    yield h
+    h.clear()  # release the 34 GB index before the next module runs
     del idx, eng, a8, sa, sb, v, l
     torch.cuda.empty_cache()
 
