@@ -11,7 +11,6 @@ The path shards two ways (no exchange on the data path for the first):
 """
 from __future__ import annotations
 
-import numpy as np
 import torch
 import torch.distributed as dist
 

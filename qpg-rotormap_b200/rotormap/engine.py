@@ -16,7 +16,7 @@ import torch
 from . import _lib
 from ._lib import Tuning, check, lib, ptr, stream_handle
 from .encoder import RopeEncoder, encode_frag_real_batch, f16_to_f8
-from .fasta import DeviceFastaFragments, FastaFragments, fasta_chunks_device, fasta_reads, fasta_reads_device
+from .fasta import DeviceFastaFragments, FastaFragments, fasta_chunks_device, fasta_reads
 
 _MODES = {"f16": _lib.SCORE_F16, "f32": _lib.SCORE_F32, "scaled": _lib.SCORE_SCALED}
 # epilogue form of the fused kernels: auto, 4 warps, or 8 warps (two column

@@ -6,14 +6,13 @@ engine_fp8.jl:654-733 (map_and_count) and RotorMap/reads/provenance.jl:46-78
 """
 from __future__ import annotations
 
-import math
 import os
 import time
 
 import numpy as np
 import torch
 
-from .engine import TopKEngine, rope_topk_stream
+from .engine import rope_topk_stream
 from .index import Index, index_database, load_index
 
 

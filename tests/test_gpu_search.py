@@ -136,7 +136,7 @@ def test_engine_rejects_bad_arguments():
     with pytest.raises(ValueError):
         rm.TopKEngine(B, k=101)
     with pytest.raises(rm.R2MError):
-        from rotormap._lib import Tuning, lib, check
+        from rotormap._lib import lib, check
         import ctypes
         h = ctypes.c_void_p()
         check(lib().r2m_engine_create(B.data_ptr(), None, 60, 100, 20, 10, 0, None, ctypes.byref(h)))

@@ -8,7 +8,6 @@ import time
 
 import numpy as np
 import pytest
-import torch
 
 import rotormap as rm
 from rotormap import serving, synth

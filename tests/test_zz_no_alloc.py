@@ -7,7 +7,6 @@ device, and hosts whose memory pool owns the device memory).  Its results must e
 keeps the previous call's contents, which must not leak into the next.
 This file is collected last so a failure here comes after every other test.
 """
-import ctypes
 
 import numpy as np
 import pytest
