@@ -484,7 +484,9 @@ constexpr int HALF_TILE = 128 * BK;  // 16 KiB
 // every PACE_EVERY tiles and, while it is more than `window` tiles ahead of
 // the slowest started pair, sleeps -- for at most PACE_CHECKS short naps.
 // Pacing only ever delays a pair a little: it never waits for a pair that is
-// not running, and it cannot stall the launch.
+// not running, nor for one more than PACE_LOST windows behind (a pair that
+// started late, e.g. on a GPU shared with other work, is outside any shared
+// L2 range and cannot be waited out), and it cannot stall the launch.
 // Same-box sweep on 65,536 reads x 16.8M columns (mean of two launches):
 // no pacing 1,761 ms; window 16 checked every 16 tiles 1,667 ms; windows of
 // 32 / 64 / 128 tiles 1,693 / 1,717 / 1,732 ms; tighter windows or checks
@@ -492,15 +494,17 @@ constexpr int HALF_TILE = 128 * BK;  // 16 KiB
 constexpr int PACE_EVERY = 16;
 constexpr int PACE_CHECKS = 16;
 constexpr int PACE_WINDOW = 16;  // tiles of 256 columns: 8 MiB of a 2048-byte index
+constexpr int PACE_LOST = 8;     // windows behind which a pair is no longer waited for
 
 __device__ __forceinline__ void pace_pair(long long *pace, int pair, int npairs, long long pos, int window) {
   volatile long long *p = pace;
   p[pair] = pos;
   for (int it = 0; it < PACE_CHECKS; ++it) {
+    const long long lost = pos - (long long)PACE_LOST * window;
     long long mn = LLONG_MAX;
     for (int q = 0; q < npairs; ++q) {
       const long long v = p[q];
-      if (v >= 0 && v < mn) mn = v;
+      if (v >= 0 && v >= lost && v < mn) mn = v;
     }
     if (pos - mn <= window) return;
     __nanosleep(1000);
