@@ -20,6 +20,10 @@
 #include <thread>
 #include <vector>
 
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
+
 #include "r2m.h"
 
 namespace r2m {
@@ -48,6 +52,40 @@ struct Lut {
   }
 };
 const Lut kLut;
+
+// 16 sequence bytes -> their 2-bit codes packed into one word (byte j at
+// bits 2j); false when the block holds a line break (the caller then walks
+// it byte by byte).  For A/C/G/T in either case ((c >> 1) ^ (c >> 2)) & 3 is
+// the code; every other byte becomes 2 (G).
+inline bool pack16(const uint8_t *q, uint32_t &out) {
+#if defined(__SSE2__)
+  const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i *>(q));
+  const __m128i brk = _mm_or_si128(_mm_cmpeq_epi8(c, _mm_set1_epi8('\n')), _mm_cmpeq_epi8(c, _mm_set1_epi8('\r')));
+  if (_mm_movemask_epi8(brk)) return false;
+  __m128i code = _mm_and_si128(_mm_xor_si128(_mm_srli_epi16(c, 1), _mm_srli_epi16(c, 2)), _mm_set1_epi8(3));
+  const __m128i lc = _mm_or_si128(c, _mm_set1_epi8(0x20));  // case fold
+  const __m128i valid =
+      _mm_or_si128(_mm_or_si128(_mm_cmpeq_epi8(lc, _mm_set1_epi8('a')), _mm_cmpeq_epi8(lc, _mm_set1_epi8('c'))),
+                   _mm_or_si128(_mm_cmpeq_epi8(lc, _mm_set1_epi8('g')), _mm_cmpeq_epi8(lc, _mm_set1_epi8('t'))));
+  code = _mm_or_si128(_mm_and_si128(valid, code), _mm_andnot_si128(valid, _mm_set1_epi8(2)));
+  // pack: byte pairs -> 4 bits, 16-bit pairs -> 8 bits, 32-bit pairs -> 16 bits
+  __m128i x = _mm_and_si128(_mm_or_si128(code, _mm_srli_epi16(code, 6)), _mm_set1_epi16(0x00FF));
+  x = _mm_and_si128(_mm_or_si128(x, _mm_srli_epi32(x, 12)), _mm_set1_epi32(0x000000FF));
+  x = _mm_or_si128(x, _mm_srli_epi64(x, 24));
+  out = ((uint32_t)_mm_cvtsi128_si32(x) & 0xFFFFu) | (((uint32_t)_mm_extract_epi16(x, 4) & 0xFFFFu) << 16);
+  return true;
+#else
+  uint32_t v = 0;
+  uint8_t any = 0;
+  for (int j = 0; j < 16; ++j) {
+    const uint8_t c = kLut.code[q[j]];
+    any |= c;
+    v |= (uint32_t)(c & 3) << (2 * j);
+  }
+  out = v;
+  return !(any & kSkip);
+#endif
+}
 
 inline bool is_rec_start(const char *d, size_t i) {
   return d[i] == '>' && (i == 0 || d[i - 1] == '\n' || d[i - 1] == '\r');
@@ -97,16 +135,8 @@ void parse_range(const char *d, size_t n, size_t lo, size_t hi, int k, Part &out
     const uint8_t *code = kLut.code;
     while (bases < k && p < e) {
       if (bases + 16 <= k && p + 16 <= e) {
-        const uint8_t *q = (const uint8_t *)d + p;
-        uint32_t v = 0;
-        uint8_t any = 0;
-#pragma GCC unroll 16
-        for (int j = 0; j < 16; ++j) {
-          uint8_t c = code[q[j]];
-          any |= c;
-          v |= (uint32_t)(c & 3) << (2 * j);
-        }
-        if (!(any & kSkip)) {
+        uint32_t v;
+        if (pack16((const uint8_t *)d + p, v)) {
           int wi = bases >> 4, sh = 2 * (bases & 15);
           w[wi] |= v << sh;
           if (sh) w[wi + 1] |= v >> (32 - sh);
