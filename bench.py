@@ -624,9 +624,12 @@ def fasta_leg(dev, n_reads: int = 400_000, seed: int = 71):
     nbytes = len(raw)
     threads = os.cpu_count() or 1
     rm.fasta_reads(raw, k=K_BASES, parts=threads)
-    t0 = time.perf_counter()
-    h = rm.fasta_reads(raw, k=K_BASES, parts=threads)
-    t_host = time.perf_counter() - t0
+    t_hosts = []
+    for _ in range(5):  # the box's host cores are shared: best and median of 5
+        t0 = time.perf_counter()
+        h = rm.fasta_reads(raw, k=K_BASES, parts=threads)
+        t_hosts.append(time.perf_counter() - t0)
+    t_host = min(t_hosts)
     d_raw = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
     for _ in range(3):
         g = rm.fasta_reads_device(raw, k=K_BASES, device=dev)
@@ -651,7 +654,8 @@ def fasta_leg(dev, n_reads: int = 400_000, seed: int = 71):
     del d_raw, g
     torch.cuda.empty_cache()
     return {"workload": f"{n_reads} reads of 150 bp, {nbytes} bytes of FASTA", "bytes": nbytes,
-            "host_native_s": t_host, "host_native_GBps": nbytes / t_host / 1e9, "host_threads": threads,
+            "host_native_s": t_host, "host_native_GBps": nbytes / t_host / 1e9,
+            "host_native_median_s": float(np.median(t_hosts)), "host_threads": threads,
             "device_c_entry_ms": ms, "device_c_entry_GBps": nbytes / ms / 1e6,
             "device_api_from_host_s": t_api, "device_api_from_host_GBps": nbytes / t_api / 1e9,
             "identical_to_host_reader": bool(same)}
