@@ -385,6 +385,60 @@ const int64_t *r2m_dreads_spans(const r2m_dreads *r);
 const uint8_t *r2m_dreads_header_blob(const r2m_dreads *r, size_t *total_len);
 void r2m_dreads_free(r2m_dreads *r);
 
+/* ------------------------------------------- reference index file (.bin) */
+
+/* The reference's index file is a Julia `Serialization` stream of one
+ * NamedTuple (save / load, RotorMap/common/dna.jl:23-34; the fields of
+ * _index_data_nt, RotorMap/index/build.jl:755-772).  These entry points read
+ * and write the subset of that format such a NamedTuple uses: Int64, Bool and
+ * String fields, arrays of bits types (UInt8, Int32, Int64, Float16, Float32,
+ * Float64, DLFP8Types.Float8_E4M3FN) and Vector{String}. */
+typedef struct r2m_jlbin r2m_jlbin;
+
+enum { R2M_JL_OTHER = 0, R2M_JL_INT = 1, R2M_JL_BOOL = 2, R2M_JL_STRING = 3, R2M_JL_ARRAY = 4,
+       R2M_JL_STRVEC = 5 };
+enum { R2M_JL_U8 = 1, R2M_JL_I32 = 2, R2M_JL_I64 = 3, R2M_JL_F16 = 4, R2M_JL_F32 = 5, R2M_JL_F64 = 6,
+       R2M_JL_E4M3 = 7 };
+
+/* One NamedTuple field.  Arrays are Julia-shaped: dims[0] is the fastest
+ * (column-major) dimension, so embeds8 (rdim, N) holds N columns of rdim
+ * bytes back to back.  A Vector{String} (R2M_JL_STRVEC) is given as its
+ * distinct strings (blob + nuniq + 1 offsets uniq_off) and, in data, one
+ * int32 index into them per element. */
+typedef struct {
+  const char *name;     /* field name, NUL-terminated */
+  int kind;             /* R2M_JL_* kind */
+  int elty;             /* R2M_JL_ARRAY element type */
+  int64_t ival;         /* R2M_JL_INT value, R2M_JL_BOOL 0/1 */
+  const char *str;      /* R2M_JL_STRING bytes (not NUL-terminated) */
+  int64_t str_len;
+  int ndims;            /* arrays: 1 or 2 */
+  int64_t dims[2];
+  const void *data;     /* array elements; STRVEC: int32 per element */
+  int64_t offset;       /* read side: byte offset of `data` in the file (-1 if none) */
+  const char *blob;     /* STRVEC distinct strings, concatenated */
+  const int64_t *uniq_off; /* STRVEC: nuniq + 1 offsets into blob */
+  int64_t nuniq;
+} r2m_jl_field;
+
+/* Replaces `load` of an index .bin (RotorMap/common/dna.jl:30-34, called by
+ * load_index, RotorMap/index/load.jl:49-73): memory-maps the file and parses
+ * the NamedTuple; array payloads point into the mapping and stay valid until
+ * r2m_jlbin_close.  R2M_EIO names the first byte the reader does not accept.
+ * r2m_jlbin_parse reads a stream already in memory (kept by the caller). */
+int r2m_jlbin_open(const char *path, r2m_jlbin **out);
+int r2m_jlbin_parse(const void *data, size_t len, r2m_jlbin **out);
+int r2m_jlbin_version(const r2m_jlbin *b);  /* the stream's format version byte */
+int r2m_jlbin_nfields(const r2m_jlbin *b);
+int r2m_jlbin_field(const r2m_jlbin *b, int i, r2m_jl_field *out);
+void r2m_jlbin_close(r2m_jlbin *b);
+/* Replaces `save` of an index (RotorMap/common/dna.jl:23-27, called by
+ * run_save, RotorMap/index/build.jl:781-795): writes the NamedTuple of
+ * `fields` in order as the stream Julia's `deserialize` reads back (Int64,
+ * Bool, String, arrays, Vector{String} with repeated strings longer than 7
+ * bytes written once and referenced after). */
+int r2m_jlbin_write(const char *path, const r2m_jl_field *fields, int nfields);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,9 +11,10 @@ from .engine import (CompactEngine, Mapper, PlainEngine, TopKBatch, TopKEngine, 
                      rope_topk_stream, rope_topk_stream_compact, topk_flow, upload_fp16_as_f8)
 from .fasta import (DeviceFastaFragments, FastaFragments, HeaderList, fasta_chunks_device, fasta_reads,
                     fasta_reads_device)
-from .index import (FP8_FORMAT, SCALED_FORMAT, Index, RefPack, build_index, build_index_packed,
-                    index_database,
-                    load_index, pack_records, pack_reference, save_index, window_positions)
+from .index import (FP8_FORMAT, ROW_FORMAT, SCALED_FORMAT, Index, RefPack, attach_genome, build_index,
+                    build_index_packed, index_database, index_to_f8, load_index, pack_records,
+                    pack_reference, save_index, window_positions)
+from . import jlbin
 from .batching import Autotuner, RaggedBatcher, bucket_rows
 from .precision import DeviceMeta, check_fp64, map_precise, rescore_fp32
 from .mapping import julia_repr_f32, map_and_count, parse_read_head, run_map, score_provenance

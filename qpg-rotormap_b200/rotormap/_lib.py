@@ -94,6 +94,13 @@ SIGNATURES = [
     ("r2m_dreads_spans", P, [P]),
     ("r2m_dreads_header_blob", P, [P, ctypes.POINTER(SZ)]),
     ("r2m_dreads_free", None, [P]),
+    ("r2m_jlbin_open", I, [ctypes.c_char_p, ctypes.POINTER(P)]),
+    ("r2m_jlbin_parse", I, [P, SZ, ctypes.POINTER(P)]),
+    ("r2m_jlbin_version", I, [P]),
+    ("r2m_jlbin_nfields", I, [P]),
+    ("r2m_jlbin_field", I, [P, I, P]),
+    ("r2m_jlbin_close", None, [P]),
+    ("r2m_jlbin_write", I, [ctypes.c_char_p, P, I]),
 ]
 
 _lib = None

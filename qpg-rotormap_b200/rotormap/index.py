@@ -3,10 +3,13 @@
 The reference index is a Julia-serialized NamedTuple (format
 "indexreal.fp8.v1": embeds8 (rdim, 2*n_frag) e4m3 columns, norms (m, 2*n_frag),
 heads, starts (1-based), strand (0 fwd / 1 rc), k, kstep, s, m, c,
-normalize).  This module keeps those fields and that column layout; on disk it
-uses a flat container (magic "R2MIDX01", a JSON header, 64-byte aligned raw
-arrays) that numpy can memory-map, because Julia's Serialization format is
-not available to a C/Python host.
+normalize).  `save_index` writes that file (the library's Serialization
+writer, csrc/jlser.cpp) and `load_index` reads it, memory-mapped, with the
+reference loader's checks; it also reads the reference's fp16/fp32 row
+layout ("indexreal.v1") and the pre-rename format tags.  A second, optional
+container (magic "R2MIDX01", a JSON header, 64-byte aligned raw arrays;
+files named *.r2mi) also keeps the packed genome that FP32 rescoring
+re-encodes windows from, which the reference's NamedTuple does not carry.
 
 Build: the host packs every record once into 2-bit words (each record starts
 on a word boundary and is followed by a zero guard word), lists the window
@@ -30,6 +33,9 @@ from ._lib import check, lib, ptr, stream_handle
 from .encoder import RopeEncoder
 
 FP8_FORMAT = "indexreal.fp8.v1"          # load.jl:31
+ROW_FORMAT = "indexreal.v1"              # load.jl:30 (fp16 / fp32 rows)
+LEGACY_FP8_FORMAT = "indexflowreal.fp8.v1"  # load.jl:33-34 (pre-rename saves)
+LEGACY_ROW_FORMAT = "indexflowreal.v1"
 SCALED_FORMAT = "indexreal.fp8scaled.v1"  # per-column scaled e4m3 (precision form)
 _MAGIC = b"R2MIDX01"
 
@@ -169,6 +175,7 @@ class Index:
     rec_nbases: np.ndarray
     batch_size: int = 8192
     scales: object = None      # (N,) float32 column scales (scaled form only)
+    rows: object = None        # row-layout .bin: Julia (N, rdim) fp16/fp32 as an (rdim, N) array
     _heads: list = field(default=None, repr=False)
 
     @property
@@ -288,13 +295,47 @@ def _host(a):
     return np.asarray(a)
 
 
-def save_index(idx: Index, path) -> None:
-    """run_save (build.jl:781-795) into the flat container (see module doc)."""
+def save_index(idx: Index, path, container: bool | None = None) -> None:
+    """run_save (build.jl:781-795): the reference's Julia-serialized
+    NamedTuple, or (container=True, or a path ending in .r2mi) the flat
+    container that also keeps the packed genome (see module doc)."""
+    if container is None:
+        container = os.fspath(path).endswith(".r2mi")
+    if container:
+        _save_container(idx, path)
+    else:
+        _save_bin(idx, path)
+
+
+def _save_bin(idx: Index, path) -> None:
+    """_index_data_nt(...; fp8 = true) + save (build.jl:755-768,
+    dna.jl:23-27): the 15 fields in the reference's order.  The scaled form
+    (a format of this library) adds its column scales as a 16th field."""
+    from . import jlbin
+    emb = _host(idx.embeds8)
+    fields = [("format", idx.format), ("source", idx.source), ("k", int(idx.k)), ("kstep", int(idx.kstep)),
+              ("s", int(idx.s)), ("m", int(idx.m)), ("c", int(idx.c)), ("normalize", int(idx.normalize)),
+              ("fp8", True), ("n_frag", int(idx.n_frag)), ("embeds8", jlbin.E4M3(emb)),
+              ("norms", np.ascontiguousarray(_host(idx.norms), dtype=np.float32)),
+              ("heads", jlbin.StrVec(list(idx.rec_heads), np.asarray(idx.col_rec, np.int32))),
+              ("starts", np.ascontiguousarray(idx.starts, dtype=np.int64)),
+              ("strand", np.ascontiguousarray(idx.strand, dtype=np.uint8))]
+    if idx.scaled:
+        fields.append(("scales", np.ascontiguousarray(_host(idx.scales), dtype=np.float32)))
+    jlbin.write_bin(path, fields)
+
+
+def _save_container(idx: Index, path) -> None:
     meta = dict(format=idx.format, source=idx.source, k=idx.k, kstep=idx.kstep, s=idx.s, m=idx.m,
                 c=idx.c, normalize=idx.normalize, fp8=True, n_frag=idx.n_frag,
                 batch_size=idx.batch_size, rec_heads=idx.rec_heads, arrays={})
     arrays = {}
     for name in _ARRAYS:
+        if getattr(idx, name) is None:
+            if name == "scales":
+                continue
+            raise ValueError(f"the container needs {name}; an index read from a reference .bin has no "
+                             "packed genome (build it from its FASTA)")
         a = _host(getattr(idx, name))
         if a is not None:
             arrays[name] = np.ascontiguousarray(a)
@@ -322,14 +363,23 @@ def save_index(idx: Index, path) -> None:
 def load_index(path, device=None, mmap: bool = True) -> Index:
     """load_index (load.jl:49-73): structural checks, normalize == 0 required.
 
-    embeds8 stays on the host (memory-mapped) unless `device` is given, in
-    which case it is uploaded once (index_database, load.jl:156-161).
+    Reads the reference's .bin (Julia-serialized NamedTuple, fp8 column or
+    fp16/fp32 row layout) or the flat container.  embeds8 stays on the host
+    (memory-mapped) unless `device` is given, in which case it is uploaded
+    once (index_database, load.jl:156-161).
     """
+    path = os.fspath(path)
     if not os.path.isfile(path):
-        raise FileNotFoundError(f"index file not found: {path}")
+        raise FileNotFoundError(f"index .bin not found: {path}")
     with open(path, "rb") as f:
-        if f.read(8) != _MAGIC:
-            raise ValueError(f"not a rotormap index container: {path}")
+        head = f.read(8)
+    from . import jlbin
+    if head[:3] == jlbin.JULIA_MAGIC:
+        return _load_bin(path, device, mmap)
+    if head != _MAGIC:
+        raise ValueError(f"not an {ROW_FORMAT}/{FP8_FORMAT} index: {path}")
+    with open(path, "rb") as f:
+        f.read(8)
         hl = int(np.frombuffer(f.read(8), np.uint64)[0])
         meta = json.loads(f.read(hl))
     base = (len(_MAGIC) + 8 + hl + 63) // 64 * 64
@@ -370,9 +420,116 @@ def load_index(path, device=None, mmap: bool = True) -> Index:
                  scales=scales)
 
 
+def _load_bin(path, device, mmap: bool) -> Index:
+    """The reference's .bin: the checks of load_index (load.jl:49-73) on the
+    NamedTuple that _index_data_nt writes (build.jl:755-772)."""
+    from . import jlbin
+    d, _ = jlbin.read_bin(path, mmap=mmap)
+    fmt = d.get("format")
+    fp8 = fmt in (FP8_FORMAT, LEGACY_FP8_FORMAT, SCALED_FORMAT)
+    if not (fp8 or fmt in (ROW_FORMAT, LEGACY_ROW_FORMAT)):
+        raise ValueError(f"not an {ROW_FORMAT}/{FP8_FORMAT} index: {path}")
+    for key in ("k", "kstep", "s", "m", "c", "normalize", "n_frag", "norms", "heads", "starts", "strand"):
+        if key not in d:
+            raise ValueError(f"index .bin lacks the field {key}: {path}")
+    if d["normalize"] != 0:
+        raise ValueError(f"mapping assumes a normalize = 0 index (got {d['normalize']}): "
+                         "unit-energy rows are what makes B's columns normalized")
+    rdim = 2 * d["m"] * 4 ** d["c"]
+    N = 2 * d["n_frag"]
+    rows = None
+    if fp8:
+        emb = d.get("embeds8")
+        if not isinstance(emb, jlbin.E4M3Array):
+            raise ValueError("embeds8 eltype mismatch")
+        if tuple(emb.shape) != (N, rdim):  # Julia (rdim, N)
+            raise ValueError("embeds8 shape mismatch")
+        emb = emb.view(np.ndarray)
+    else:
+        rows = d.get("embeds")
+        want = np.float16 if d.get("fp16", False) else np.float32
+        if not isinstance(rows, np.ndarray) or rows.dtype != want:
+            raise ValueError("embeds eltype mismatch")
+        if tuple(rows.shape) != (rdim, N):  # Julia (N, rdim), column-major
+            raise ValueError("embeds shape mismatch")
+        emb = None
+    heads, starts, strand, norms = d["heads"], d["starts"], d["strand"], d["norms"]
+    if not (isinstance(heads, jlbin.StrVec) and len(heads) == starts.shape[0] == strand.shape[0] == N):
+        raise ValueError("meta length mismatch")
+    if tuple(norms.shape) != (N, d["m"]):
+        raise ValueError("norms shape mismatch")
+    scales = d.get("scales") if fmt == SCALED_FORMAT else None
+    idx = Index(format=SCALED_FORMAT if fmt == SCALED_FORMAT else FP8_FORMAT, source=d.get("source", ""),
+                k=d["k"], kstep=d["kstep"], s=d["s"], m=d["m"], c=d["c"], normalize=0, n_frag=d["n_frag"],
+                embeds8=emb, norms=norms, rec_heads=list(heads.uniq), col_rec=heads.idx,
+                starts=starts, strand=strand, col_pos=None, genome=None,
+                rec_word_off=np.zeros(0, np.int64), rec_nbases=np.zeros(0, np.int64), scales=scales)
+    idx.rows = rows
+    if device is not None:
+        idx.embeds8 = index_database(idx, device)
+        if scales is not None:
+            idx.scales = torch.from_numpy(np.ascontiguousarray(scales)).to(device)
+    return idx
+
+
+def attach_genome(idx: Index, fasta=None) -> Index:
+    """Give an index read from a reference .bin (which stores no packed
+    genome) the packed records and per-column genome positions that FP32
+    rescoring re-encodes windows from: the source FASTA (`fasta`, default
+    the index's `source` field) is packed again and each column's record is
+    found by its verbatim header."""
+    src = fasta if fasta is not None else idx.source
+    if not src or not os.path.isfile(os.fspath(src)):
+        raise ValueError(f"the index's source FASTA is not available ({src!r}); pass fasta=")
+    pack = pack_reference(src)
+    where = {}
+    for r, h in enumerate(pack.heads):
+        if h in where:
+            raise ValueError(f"duplicate record header {h!r} in {src}: columns cannot be placed")
+        where[h] = r
+    try:
+        rec_of = np.array([where[h] for h in idx.rec_heads], np.int64)
+    except KeyError as e:
+        raise ValueError(f"record {e.args[0]!r} of the index is not in {src}") from None
+    col_rec = np.asarray(idx.col_rec, np.int64)
+    recs = rec_of[col_rec]
+    starts0 = np.asarray(idx.starts, np.int64) - 1
+    if np.any(starts0 < 0) or np.any(starts0 + idx.k > pack.nbases[recs]):
+        raise ValueError(f"index windows do not fit the records of {src}")
+    idx.col_pos = 16 * pack.word_off[recs] + starts0
+    idx.genome, idx.rec_word_off, idx.rec_nbases = pack.words, pack.word_off, pack.nbases
+    return idx
+
+
+def index_to_f8(rows, device=None, block: int = 1 << 16, stream=None) -> torch.Tensor:
+    """index_to_f8 (load.jl:75-97): the row-layout index (Julia (N, rdim)
+    fp16/fp32, here its column-major bytes as an (rdim, N) array) -> the
+    e4m3 database B, block by block: H2D, transpose, quantise (the library's
+    cvt.rn.satfinite conversion, fp16 -> fp32 -> e4m3 like the reference)."""
+    _lib.require_device()
+    rdim, N = rows.shape
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    B = torch.empty((N, rdim), dtype=torch.uint8, device=dev)
+    conv = lib().r2m_f16_to_e4m3 if rows.dtype == np.float16 else lib().r2m_f32_to_e4m3
+    st = stream if stream is not None else torch.cuda.current_stream(dev)
+    with torch.cuda.stream(st):
+        for j0 in range(0, N, block):
+            j1 = min(N, j0 + block)
+            blk = torch.from_numpy(np.ascontiguousarray(rows[:, j0:j1])).to(dev, non_blocking=False)
+            t = blk.t().contiguous()
+            check(conv(ptr(B[j0:j1]), ptr(t), t.numel(), st.cuda_stream))
+    st.synchronize()
+    return B
+
+
 def index_database(idx: Index, device=None) -> torch.Tensor:
-    """index_database (load.jl:156-161): the resident e4m3 database B on the GPU."""
+    """index_database (load.jl:156-161): the resident e4m3 database B on the
+    GPU -- one H2D for the fp8 layout, index_to_f8 for the row layout."""
     if isinstance(idx.embeds8, torch.Tensor) and idx.embeds8.is_cuda:
         return idx.embeds8
     dev = device if device is not None else "cuda"
+    if idx.embeds8 is None:
+        if getattr(idx, "rows", None) is None:
+            raise ValueError("index holds no embeddings")
+        return index_to_f8(idx.rows, dev)
     return torch.from_numpy(np.ascontiguousarray(idx.embeds8)).to(dev)

@@ -19,6 +19,9 @@ class DeviceMeta:
 
     def __init__(self, idx, device=None, genome: torch.Tensor | None = None):
         dev = device or (idx.embeds8.device if isinstance(idx.embeds8, torch.Tensor) else "cuda")
+        if genome is None and idx.genome is None:
+            from .index import attach_genome
+            attach_genome(idx)  # an index read from a reference .bin: pack its source FASTA
         if genome is None:
             genome = torch.from_numpy(np.ascontiguousarray(idx.genome).view(np.int32)).to(dev)
         self.genome = genome

@@ -130,6 +130,51 @@ def test_index_save_load_map_round_trip(fixture, tmp_path):
     assert np.array_equal(a[0].locs, b[0].locs) and np.array_equal(a[0].vals, b[0].vals)
 
 
+def test_reference_bin_round_trip_maps(fixture, tmp_path):
+    """The reference's index file (Julia-serialized NamedTuple, written by
+    save_index): load_index memory-maps it, uploads embeds8 once and the
+    search, the table and the rescoring meta match the built index."""
+    heads, recs, re, idx = fixture
+    path = tmp_path / "g.indexreal_fp8.bin"
+    idx.save(path)
+    back = rm.load_index(str(path), device="cuda")
+    assert back.format == rm.FP8_FORMAT and back.N == idx.N and back.heads == idx.heads
+    assert torch.equal(back.embeds8, idx.embeds8)
+    assert np.array_equal(np.asarray(back.starts), idx.starts) and np.array_equal(np.asarray(back.strand), idx.strand)
+    p, _, _ = _reads_file(tmp_path, heads, recs, 200, 0.05, 21, "rb.fa")
+    a = list(rm.rope_topk_stream(re, str(p), idx.embeds8, k=20))
+    b = list(rm.rope_topk_stream(re, str(p), back.embeds8, k=20))
+    assert np.array_equal(a[0].locs, b[0].locs) and np.array_equal(a[0].vals, b[0].vals)
+    # run_map straight from the .bin path (the tools/map.jl contract)
+    out_a, out_b = tmp_path / "a.maps", tmp_path / "b.maps"
+    rm.run_map(idx, str(p), str(out_a), topk=5)
+    rm.run_map(str(path), str(p), str(out_b), topk=5)
+    assert out_a.read_bytes() == out_b.read_bytes()
+    # the packed genome for rescoring is rebuilt from the source FASTA
+    fa = tmp_path / "g.fa"
+    fa.write_bytes(synth.genome_fasta(heads, recs))
+    rm.attach_genome(back, str(fa))
+    assert np.array_equal(back.col_pos, idx.col_pos)
+
+
+def test_row_layout_bin_quantises_like_the_reference(tmp_path):
+    """An "indexreal.v1" fp16 row-layout file: index_database builds B with
+    H2D + transpose + e4m3(fp32(fp16)) (index_to_f8, load.jl:75-97)."""
+    rng = np.random.default_rng(12)
+    N, m, c = 70_000, 1, 2
+    rdim = 2 * m * 4 ** c
+    rows = (rng.standard_normal((rdim, N)) * 0.3).astype(np.float16)  # Julia (N, rdim) column-major
+    path = tmp_path / "rows.bin"
+    rm.jlbin.write_bin(path, [("format", "indexreal.v1"), ("source", "x.fa"), ("k", 20), ("kstep", 2),
+                              ("s", 3), ("m", m), ("c", c), ("normalize", 0), ("fp16", True), ("n_frag", N // 2),
+                              ("embeds", rows), ("norms", np.ones((N, m), np.float32)),
+                              ("heads", [">a"] * N), ("starts", np.arange(1, N + 1)),
+                              ("strand", np.zeros(N, np.uint8))])
+    idx = rm.load_index(str(path), device="cuda")
+    want = orc.f32_to_e4m3(rows.T.astype(np.float32))
+    assert np.array_equal(idx.embeds8.cpu().numpy(), want)
+
+
 def test_scaled_index_maps_as_well(tmp_path):
     heads = [">s1", ">s2"]
     recs = synth.random_genome([50_000, 30_000], seed=2)
