@@ -40,12 +40,8 @@ KSTEP = 15
 Q = 65_536
 N_COLS = 16_777_216
 TOPK = 20
-# DRAM bytes (read + write) of one fused launch at the default workload
-# (65,536 reads x 16,777,216 columns): the mean over the 9 launches of a
-# one-pass ncu capture of the bench command
-# (profiles/k_gemm_topk2_65536x16777216_dram.md)
-FUSED_DRAM_BYTES = 138_477_900_000 + 90_320_000
 ERR = 0.05
+TIE_F16 = 1e-3  # one fp16 step of a score near 1 (2^-10)
 GENOME_SEED, READ_SEED = 7, 11
 METRIC = "reads/s on 1 B200 at top-20 recall = ref, serving vs plain; p50/p99 latency"
 
@@ -281,11 +277,23 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31):
     out["plain_fused_kernel"] = stats([p[0] for p in fres], t0)
     eng.close()
     out["serving_vs_plain"] = out["serving"]["reads_per_s"] / out["plain_reference_engine"]["reads_per_s"]
-    # recall of the served top-20 against the reference-structured engine
-    ov, same = [], 0
-    for (v, l), (_, pv, pl) in zip(res, pres):
-        ov.append(np.mean([len(set(a) & set(b)) / TOPK for a, b in zip(l, pl)]))
-    out["top20_recall_vs_plain_reference"] = float(np.average(ov, weights=sizes))
+    # top-20 recall against the reference-structured engine.  That engine
+    # keeps an arbitrary one of tied locations (its segmented top-k), so a
+    # served location that is not in its list counts as recalled when it ties
+    # the list's 20th value within one fp16 step (both paths round fp32 sums
+    # to fp16); `untied_misses` counts the served locations that are neither.
+    sv = np.concatenate([v for v, _ in res]).astype(np.float32)
+    sl = np.concatenate([l for _, l in res])
+    pv = np.concatenate([p[1] for p in pres]).astype(np.float32)
+    pl = np.concatenate([p[2] for p in pres])
+    inset = np.zeros(sl.shape, bool)
+    for r0 in range(0, sl.shape[0], 65536):
+        inset[r0:r0 + 65536] = (sl[r0:r0 + 65536, :, None] == pl[r0:r0 + 65536, None, :]).any(axis=2)
+    tied = ~inset & (sv >= pv[:, -1:] - TIE_F16)
+    out["top20_recall_vs_plain_reference"] = float((inset | tied).mean())
+    out["top20_set_overlap_vs_plain_reference"] = float(inset.mean())
+    out["untied_misses"] = int((~inset & ~tied).sum())
+    out["tie_tolerance"] = TIE_F16
     # provenance: a read maps if a top-20 window overlaps its true position
     hit = 0
     recmap = idx.col_rec
@@ -401,7 +409,7 @@ def batching_leg(dev, n_requests: int, seed: int = 61):
     del words
     total = int(counts.sum())
     eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=rm.bucket_rows(total), score="f16")
-    tuner = rm.Autotuner(proxy_cols=1 << 20)
+    tuner = rm.Autotuner()  # no cache file: this run pays the tuning
     b = rm.RaggedBatcher(eng, re, total, tuner=tuner, use_graphs=True)
     t0 = time.perf_counter()
     b.run(reqs)  # tune + capture + first replay
@@ -409,8 +417,21 @@ def batching_leg(dev, n_requests: int, seed: int = 61):
     t0 = time.perf_counter()
     res = b.run(reqs)
     t_ragged = time.perf_counter() - t0
+    tuned = {k: tuner.last[k] for k in ("splits", "ctas", "kernel", "epilogue", "pace", "kt")}
+    default = {"splits": 0, "ctas": 0, "kernel": "auto", "epilogue": "auto", "pace": 0, "kt": 0}
+    if tuned == default:
+        t_untuned = t_ragged  # the tuner kept the built-in schedule
+    else:  # the same graph-replayed launch with the built-in schedule
+        eng.set_tuning(0, 0, kernel="auto", epilogue="auto", pace=0, kt=0)
+        bu = rm.RaggedBatcher(eng, re, total, tuner=None, use_graphs=True)
+        bu.run(reqs)
+        t0 = time.perf_counter()
+        ru = bu.run(reqs)
+        t_untuned = time.perf_counter() - t0
+        assert all(np.array_equal(a[1], c[1]) for a, c in zip(res, ru)), "schedules changed the results"
+        del bu
     # one request at a time (encode + search + D2H per request, synchronous)
-    eng.set_tuning(0, 0)
+    eng.set_tuning(0, 0, kernel="auto", epilogue="auto", pace=0, kt=0)
     st = torch.cuda.current_stream()
     t0 = time.perf_counter()
     for w in reqs:
@@ -420,15 +441,17 @@ def batching_leg(dev, n_requests: int, seed: int = 61):
         v.cpu(), l.cpu()
     torch.cuda.synchronize()
     t_each = time.perf_counter() - t0
-    s_best = tuner.cache[next(iter(tuner.cache))]
     out = {"workload": f"100 Mbp genome at k=100 kstep=10 -> N={idx.N} columns, {n_requests} requests "
                        f"(log-uniform 1..50000 reads, total {total}), lengths lognormal median 150 in [100,250] "
                        f"trimmed to 100, subs U[0,0.15], top-20, f16 scores",
            "index_cols": idx.N, "requests": n_requests, "reads": total,
            "ragged_graph_reads_per_s": total / t_ragged, "per_request_reads_per_s": total / t_each,
            "speedup": t_each / t_ragged, "first_run_s": t_first, "launch_sets": 1,
-           "autotuned": {"splits": s_best[0], "ctas": s_best[1],
-                         "epilogue": s_best[2] if len(s_best) > 2 else "auto", "candidates": tuner.log}}
+           "untuned_reads_s": total / t_untuned, "tuned_vs_untuned": t_untuned / t_ragged,
+           "tuning_cost_frac": tuner.last["tune_s"] / t_ragged,
+           "autotuned": {"chosen": tuned, "tune_s": tuner.last["tune_s"], "proxy_cols": tuner.last["proxy_cols"],
+                         "proxy_default_ms": tuner.last["default_ms"], "proxy_best_ms": tuner.last["ms"],
+                         "candidates": tuner.log}}
     eng.close()
     del idx, eng, b
     torch.cuda.empty_cache()
@@ -664,6 +687,54 @@ def fasta_leg(dev, n_reads: int = 400_000, seed: int = 71):
 # ---------------------------------------------------------------- GPU leg
 
 
+def _r(x, nd=4):
+    return None if x is None else float(f"{x:.{nd}g}")
+
+
+def summary(line: dict) -> dict:
+    """The figures of every leg in one compact object (printed last)."""
+    out = {"headline_reads_s": _r(line["value"]), "e2e_reads_s": _r(line["e2e"]["value"]),
+           "gemm_tflops": _r(line["roofline"]["achieved"]), "gemm_frac_of_2x_bf16": _r(line["roofline"]["frac"], 3),
+           "encoder_gbs": _r(line["encoder"]["achieved_gbs"]),
+           "encoder_frac_hbm": _r(line["encoder"]["achieved_gbs"] / line["encoder"]["peak_gbs"], 3)}
+    if "tensor_pipe" in line["roofline"]:
+        out["tensor_pipe_est"] = _r(line["roofline"]["tensor_pipe"].get("est_active_frac"), 3)
+    sv = line.get("serving")
+    if sv:
+        out["C4_serving"] = {"reads_s": _r(sv["serving"]["reads_per_s"]), "p50_s": _r(sv["serving"]["p50_s"], 3),
+                             "p99_s": _r(sv["serving"]["p99_s"], 3),
+                             "vs_plain_reference_engine": _r(sv["serving_vs_plain"], 3),
+                             "vs_plain_fused_kernel": _r(sv["serving"]["reads_per_s"] /
+                                                         sv["plain_fused_kernel"]["reads_per_s"], 3),
+                             "recall_vs_plain_ties": _r(sv["top20_recall_vs_plain_reference"], 6),
+                             "untied_misses": sv["untied_misses"], "reads": sv["reads"]}
+    pr = line.get("precision")
+    if pr:
+        fc = pr["fp64_check"]
+        out["C2_precision"] = {"reads": pr["reads"], "reads_s": _r(pr["reads_per_s"]),
+                               "sampled_rows": fc["sampled_rows"],
+                               "recall_fp8": _r(fc["top20_recall_fp8"], 4),
+                               "recall_fp32": _r(fc["top20_recall_fp32_rescored"], 4),
+                               "err_fp8_max": _r(fc["score_abs_err_fp8"]["max"], 3),
+                               "err_fp32_max": _r(fc["score_abs_err_fp32"]["max"], 3)}
+    bt = line.get("batching")
+    if bt:
+        out["C3_batching"] = {"requests": bt["requests"], "reads": bt["reads"],
+                              "ragged_reads_s": _r(bt["ragged_graph_reads_per_s"]),
+                              "per_request_reads_s": _r(bt["per_request_reads_per_s"]),
+                              "speedup": _r(bt["speedup"], 3), "first_run_s": _r(bt["first_run_s"], 3)}
+        for key in ("untuned_reads_s", "tuned_vs_untuned", "tuning_cost_frac"):
+            if key in bt:
+                out["C3_batching"][key] = _r(bt[key], 3)
+    fa = line.get("fasta_reader")
+    if fa:
+        out["fasta_GBps"] = {k[:-5]: _r(v, 3) for k, v in fa.items()
+                             if isinstance(v, (int, float)) and k.endswith("_GBps")}
+    if line.get("cpu_baseline"):
+        out["cpu_baseline_reads_s"] = _r(line["cpu_baseline"]["value"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -682,9 +753,9 @@ def main():
     ap.add_argument("--no-compact", action="store_true", help="skip the host-ring engine leg")
     ap.add_argument("--no-map", action="store_true", help="skip the run_map end-to-end leg")
     ap.add_argument("--no-gemm-bar", action="store_true", help="skip the cuBLASLt fp8 GEMM bar")
-    ap.add_argument("--batching-requests", type=int, default=48)
-    ap.add_argument("--precision-reads", type=int, default=100_000)
-    ap.add_argument("--precision-sample", type=int, default=1000)
+    ap.add_argument("--batching-requests", type=int, default=256)
+    ap.add_argument("--precision-reads", type=int, default=1_000_000)
+    ap.add_argument("--precision-sample", type=int, default=10_000)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -795,12 +866,10 @@ def main():
                        "l2": "inputs > L2 (34 GB index streamed every step)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": FUSED_DRAM_BYTES if (args.ncols == N_COLS and nq == Q) else None,
+                         "traffic": None,
                          "traffic_algorithmic": nq * re.rdim + N * re.rdim,
-                         "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                                         "workload (ncu, 1 pass; profiles/k_gemm_topk2_65536x16777216_dram.md): "
-                                         "the index read ~4x (once per wave of paced CTA pairs, each index "
-                                         "tile shared through L2 within a wave), ~1.2% of HBM",
+                         "traffic_note": "not measured in this run: DRAM bytes come from an ncu capture, "
+                                         "which a timed run cannot carry",
                          "kernel": ("k_gemm_topk2 (CTA-pair tcgen05 fp8 GEMM + fused top-20)" if nq > 128 else
                                     "k_gemm_topk (single-CTA tcgen05 fp8 GEMM + fused top-20)"),
                          "peak_basis": f"dense fp8 = 2 x {basis} sustained bf16 "
@@ -837,6 +906,7 @@ def main():
             line["run_map"] = map_leg(dev)
         if world == 1 and not args.no_gemm_bar:
             line["gemm_bar"] = gemm_bar_leg(dev)
+        line["summary"] = summary(line)  # last key: the tail of the printed line
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

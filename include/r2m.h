@@ -139,7 +139,10 @@ typedef struct {
                       reserved[3]: pacing of the CTA-pair kernel, 0 default
                       (a pair naps while it is more than 16 column tiles
                       ahead of the slowest pair, so the pairs share index
-                      tiles through L2), > 0 that window in tiles, < 0 off */
+                      tiles through L2), > 0 that window in tiles, < 0 off;
+                      reserved[4]: top-k reservoir size per row, 0 auto
+                      (the smallest of 8/16/20/32/64 that holds k), else one
+                      of those sizes (ignored when smaller than k) */
 } r2m_tuning;
 
 /* Replaces TopKEngine(B; k, w, rows_cap, segs, engine, cout)
@@ -185,20 +188,31 @@ int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A,
  * device memory, so a side allocation can fail.  No counterpart in
  * the reference.  Takes the engine's arguments directly (B, scaleB, rdim, N,
  * k, score_mode as r2m_engine_create; A, scaleA, nb, outputs as
- * r2m_batch_gemm_topk) and calls no cudaMalloc/cudaFree: the split scratch
- * is a 32 MiB array inside the library that every GPU loading the library
- * holds until exit.  Limit: ceil(nb/128)*128 rows x the top-k list size
- * (k rounded up to 8/16/20/32/64) x 8 bytes must fit 32 MiB (nb <= 209,664
- * at k = 20); larger nb returns R2M_EINVAL.  The first call on a device looks
- * up the array's address and should come before any stream capture.  All
- * calls share the array: calls that overlap on the GPU (other streams,
- * other threads) race and must be serialized by the caller.  A device-side
- * wait that gave up marks every output row with NaN values and location -1. */
+ * r2m_batch_gemm_topk) and calls no cudaMalloc/cudaFree: the pacing slots and
+ * the split scratch are a 32 MiB array inside the library that every GPU
+ * loading the library holds until exit.  It runs the engine's automatic
+ * schedule (CTA pairs above 128 reads, paced), with the column splits cut to
+ * what the array holds, so its results equal an automatic engine's.  Limit:
+ * ceil(nb/256)*256 rows x the top-k list size (k rounded up to
+ * 8/16/20/32/64) x 8 bytes must fit 32 MiB less 8 KiB (nb <= 209,664 at
+ * k = 20); larger nb returns R2M_EINVAL.  The first call on a device (and
+ * the first after a device reset, which loads the array anew) looks up the
+ * array's address and should come before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialized by the caller.  A device-side wait
+ * that gave up marks every output row with NaN values and location -1. */
 int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_scaleB,
                                 int rdim, int64_t N, const uint8_t *d_A,
                                 const float *d_scaleA, int nb, int k,
                                 int score_mode, float *d_vals,
                                 int32_t *d_locs, r2m_stream_t stream);
+/* Self-check of the allocation-free path's give-up handling, without a
+ * fault: the kernels' bounded wait (limit_cycles SM clocks, <= 4e9) on an
+ * mbarrier that nothing arrives on gives up and records its code in that
+ * path's error word, then the pass that marks a failed search's rows writes
+ * NaN / -1 into the (nb, k) outputs.  No reference counterpart. */
+int r2m_selftest_noalloc_timeout(int64_t limit_cycles, int nb, int k, float *d_vals, int32_t *d_locs,
+                                 r2m_stream_t stream);
 
 /* ------------------------------------------------------- precision form */
 
@@ -276,7 +290,8 @@ typedef struct r2m_text r2m_text;
  * heads: nb headers, each followed by '\n'; strand / starts (1-based) /
  * col_rec: per-column index tables; rec_names: the record names (first
  * header token without '>'), each followed by '\n'.  nthreads host threads.
- * Free the text with r2m_text_free. */
+ * A location of -1 (the rows of an allocation-free search whose device-side
+ * wait gave up) returns R2M_ETIMEOUT.  Free the text with r2m_text_free. */
 int r2m_format_table(const float *vals, const int32_t *locs, int64_t nb, int k, const char *heads,
                      size_t heads_len, const uint8_t *strand, const int64_t *starts, const int32_t *col_rec,
                      int64_t ncols, const char *rec_names, size_t rec_names_len, int nthreads, r2m_text **out);

@@ -128,6 +128,12 @@ __global__ void k_selftest_wait(long long limit, int arrive, uint32_t *err) {
   __syncthreads();
 }
 
+int launch_selftest_wait(long long limit, int arrive, uint32_t *err, cudaStream_t st) {
+  k_selftest_wait<<<1, 32, 0, st>>>(limit, arrive ? 1 : 0, err);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
+
 }  // namespace r2m
 
 extern "C" {

@@ -47,6 +47,10 @@ cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t st);
 int device_error_word(uint32_t **out);
 // Reads and clears the error word after synchronizing `stream`.
 int check_device_error(cudaStream_t stream, const char *what);
+// One CTA's bounded wait (limit in SM clocks) on an mbarrier that nothing
+// arrives on (arrive = 0) or that it completed itself (arrive = 1); a wait
+// that gives up writes its code to *err.
+int launch_selftest_wait(long long limit, int arrive, uint32_t *err, cudaStream_t st);
 
 // ------------------------------------------------------------ device side
 

@@ -927,12 +927,86 @@ static int launch_gemm2(const CUtensorMap &mA, const CUtensorMap &mB, const Gemm
   return R2M_OK;
 }
 
+// Reservoir size of an engine: the smallest of 8/16/20/32/64 that holds k,
+// or tuning.reserved[4] when that is one of them and holds k.
+static int kt_for(int k, const r2m_tuning *tune) {
+  const int r = tune ? tune->reserved[4] : 0;
+  if ((r == 8 || r == 16 || r == 20 || r == 32 || r == 64) && r >= k) return r;
+  return pick_kt(k);
+}
+
+// Load every fused-kernel instance once per device (and set its shared-
+// memory limit) so that no kernel is first loaded while a stream is being
+// captured into a graph.
+static int preload_kernels() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  R2M_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return R2M_OK;
+#define R2M_PRELOAD1(KT, H)                                                                    \
+  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk<KT, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                (int)gemm_smem_bytes(H)))
+#define R2M_PRELOAD2(KT, H)                                                                     \
+  R2M_CUDA(cudaFuncSetAttribute(k_gemm_topk2<KT, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                (int)gemm2_smem_bytes(H)))
+  R2M_PRELOAD1(8, 1); R2M_PRELOAD1(16, 1); R2M_PRELOAD1(20, 1); R2M_PRELOAD1(32, 1); R2M_PRELOAD1(64, 1);
+  R2M_PRELOAD1(8, 2); R2M_PRELOAD1(16, 2); R2M_PRELOAD1(20, 2); R2M_PRELOAD1(32, 2);
+  R2M_PRELOAD2(8, 1); R2M_PRELOAD2(16, 1); R2M_PRELOAD2(20, 1); R2M_PRELOAD2(32, 1); R2M_PRELOAD2(64, 1);
+  R2M_PRELOAD2(8, 2); R2M_PRELOAD2(16, 2); R2M_PRELOAD2(20, 2); R2M_PRELOAD2(32, 2);
+#undef R2M_PRELOAD1
+#undef R2M_PRELOAD2
+  cudaFuncAttributes fa;
+  R2M_CUDA(cudaFuncGetAttributes(&fa, k_merge_splits));
+  done[dev] = true;
+  return R2M_OK;
+}
+
 // Which kernel a batch of nb reads runs on: 1 = one CTA per 128-read tile,
 // 2 = CTA pairs per 256-read tile.  mode 0 (auto) uses pairs above 128 reads.
 static int kernel_kind(int mode, int nb) {
   if (mode == 1) return 1;
   if (mode == 2) return 2;
   return nb > BM ? 2 : 1;
+}
+
+// Launch the fused kernel of `kind` (1 single-CTA, 2 CTA pairs) with
+// `halves` epilogue halves for the reservoir size KT.
+static int dispatch_gemm(int kind, int halves, int KT, const CUtensorMap &mA, const CUtensorMap &mB,
+                         const CUtensorMap &mB128, const GemmArgs &g, int ctas, cudaStream_t st) {
+  if (kind == 2) {
+    if (halves == 2) {
+      switch (KT) {
+        case 8: return launch_gemm2<8, 2>(mA, mB128, g, ctas, st);
+        case 16: return launch_gemm2<16, 2>(mA, mB128, g, ctas, st);
+        case 20: return launch_gemm2<20, 2>(mA, mB128, g, ctas, st);
+        default: return launch_gemm2<32, 2>(mA, mB128, g, ctas, st);
+      }
+    }
+    switch (KT) {
+      case 8: return launch_gemm2<8, 1>(mA, mB128, g, ctas, st);
+      case 16: return launch_gemm2<16, 1>(mA, mB128, g, ctas, st);
+      case 20: return launch_gemm2<20, 1>(mA, mB128, g, ctas, st);
+      case 32: return launch_gemm2<32, 1>(mA, mB128, g, ctas, st);
+      default: return launch_gemm2<64, 1>(mA, mB128, g, ctas, st);
+    }
+  }
+  if (halves == 2) {
+    switch (KT) {
+      case 8: return launch_gemm<8, 2>(mA, mB, g, ctas, st);
+      case 16: return launch_gemm<16, 2>(mA, mB, g, ctas, st);
+      case 20: return launch_gemm<20, 2>(mA, mB, g, ctas, st);
+      default: return launch_gemm<32, 2>(mA, mB, g, ctas, st);
+    }
+  }
+  switch (KT) {
+    case 8: return launch_gemm<8, 1>(mA, mB, g, ctas, st);
+    case 16: return launch_gemm<16, 1>(mA, mB, g, ctas, st);
+    case 20: return launch_gemm<20, 1>(mA, mB, g, ctas, st);
+    case 32: return launch_gemm<32, 1>(mA, mB, g, ctas, st);
+    default: return launch_gemm<64, 1>(mA, mB, g, ctas, st);
+  }
 }
 
 // Progress slots for pair pacing (one per CTA pair of a launch).
@@ -1010,6 +1084,7 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || (reinterpret_cast<uintptr_t>(d_scaleB) & 15) == 0,
               "scaleB must be 16-byte aligned");
   int rc = r2m_device_check();
+  if (!rc) rc = preload_kernels();
   if (rc) return rc;
   r2m_engine *e = new r2m_engine();
   e->B = d_B;
@@ -1018,7 +1093,7 @@ extern "C" int r2m_engine_create(const uint8_t *d_B, const float *d_scaleB, int 
   e->N = N;
   e->N_cap = N;
   e->k = k;
-  e->KT = pick_kt(k);
+  e->KT = kt_for(k, tune);
   e->rows_cap = rows_cap;
   e->score_mode = score_mode;
   e->ctas = (tune && tune->ctas > 0) ? tune->ctas : sm_count();
@@ -1086,12 +1161,13 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
   const int ctas = tune->ctas > 0 ? tune->ctas : sm_count();
   const int forced = tune->splits > 0 ? tune->splits : 0;
   const int mode = (tune->reserved[1] >= 0 && tune->reserved[1] <= 2) ? tune->reserved[1] : 0;
-  size_t lists = lists_needed(eng->rows_cap, eng->n_tiles, ctas, forced, mode, eng->KT);
-  if (lists > eng->part_lists) {  // grow the split workspace
+  const int KT = kt_for(eng->k, tune);
+  size_t lists = lists_needed(eng->rows_cap, eng->n_tiles, ctas, forced, mode, KT);
+  if (lists * KT > eng->part_lists * eng->KT) {  // grow the split workspace
     float *pv = nullptr;
     int *pc = nullptr;
-    cudaError_t ce = cudaMalloc(&pv, lists * eng->KT * sizeof(float));
-    if (ce == cudaSuccess) ce = cudaMalloc(&pc, lists * eng->KT * sizeof(int));
+    cudaError_t ce = cudaMalloc(&pv, lists * KT * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMalloc(&pc, lists * KT * sizeof(int));
     if (ce != cudaSuccess) {
       cudaFree(pv);
       return fail(R2M_ENOMEM, "engine workspace allocation failed");
@@ -1102,7 +1178,10 @@ extern "C" int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune) {
     eng->part_vals = pv;
     eng->part_cols = pc;
     eng->part_lists = lists;
+  } else {
+    eng->part_lists = eng->part_lists * eng->KT / KT;  // the same bytes hold more, shorter lists
   }
+  eng->KT = KT;
   eng->ctas = ctas;
   eng->forced_splits = forced;
   eng->mode = mode;
@@ -1186,41 +1265,7 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
     g.pace_window = eng->pace_window;
   }
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[0], st));
-  if (kind == 2) {
-    if (halves == 2) {
-      switch (eng->KT) {
-        case 8: rc = launch_gemm2<8, 2>(mapA, eng->mapB128, g, ctas, st); break;
-        case 16: rc = launch_gemm2<16, 2>(mapA, eng->mapB128, g, ctas, st); break;
-        case 20: rc = launch_gemm2<20, 2>(mapA, eng->mapB128, g, ctas, st); break;
-        default: rc = launch_gemm2<32, 2>(mapA, eng->mapB128, g, ctas, st); break;
-      }
-    } else {
-      switch (eng->KT) {
-        case 8: rc = launch_gemm2<8, 1>(mapA, eng->mapB128, g, ctas, st); break;
-        case 16: rc = launch_gemm2<16, 1>(mapA, eng->mapB128, g, ctas, st); break;
-        case 20: rc = launch_gemm2<20, 1>(mapA, eng->mapB128, g, ctas, st); break;
-        case 32: rc = launch_gemm2<32, 1>(mapA, eng->mapB128, g, ctas, st); break;
-        default: rc = launch_gemm2<64, 1>(mapA, eng->mapB128, g, ctas, st); break;
-      }
-    }
-  } else {
-    if (halves == 2) {
-      switch (eng->KT) {
-        case 8: rc = launch_gemm<8, 2>(mapA, eng->mapB, g, ctas, st); break;
-        case 16: rc = launch_gemm<16, 2>(mapA, eng->mapB, g, ctas, st); break;
-        case 20: rc = launch_gemm<20, 2>(mapA, eng->mapB, g, ctas, st); break;
-        default: rc = launch_gemm<32, 2>(mapA, eng->mapB, g, ctas, st); break;
-      }
-    } else {
-      switch (eng->KT) {
-        case 8: rc = launch_gemm<8, 1>(mapA, eng->mapB, g, ctas, st); break;
-        case 16: rc = launch_gemm<16, 1>(mapA, eng->mapB, g, ctas, st); break;
-        case 20: rc = launch_gemm<20, 1>(mapA, eng->mapB, g, ctas, st); break;
-        case 32: rc = launch_gemm<32, 1>(mapA, eng->mapB, g, ctas, st); break;
-        default: rc = launch_gemm<64, 1>(mapA, eng->mapB, g, ctas, st); break;
-      }
-    }
-  }
+  rc = dispatch_gemm(kind, halves, eng->KT, mapA, eng->mapB, eng->mapB128, g, ctas, st);
   if (rc) return rc;
   if (eng->timing) R2M_CUDA(cudaEventRecord(eng->ev[1], st));
   const int warps = 8;
@@ -1252,36 +1297,71 @@ extern "C" int r2m_engine_kernel_ms(r2m_engine *eng, float *gemm_ms, float *merg
 // batch: a serving loop where a cudaMalloc would synchronize the device and
 // stall other streams, or a host whose memory pool (CUDA.jl's, PyTorch's
 // caching allocator) already owns the free device memory, so a side
-// allocation can fail.  This entry point needs no engine: the per-split
-// partial top-k lists live in the file-scope array below, whose device
-// address is looked up with cudaGetSymbolAddress by the first call on each
-// device (so that first call should come before any stream capture).  Every
-// GPU that loads this library holds the array (kNoAllocScratchBytes) until
-// the process exits; all calls share it, so calls that overlap on the GPU
-// race.
+// allocation can fail.  This entry point needs no engine: the pacing slots
+// and the per-split partial top-k lists live in the file-scope array below,
+// whose device address is looked up with cudaGetSymbolAddress by the first
+// call on each device (so that first call should come before any stream
+// capture) and again whenever the device's current context is a different
+// one (after a cudaDeviceReset the module, and with it the array, is loaded
+// anew).  Every GPU that loads this library holds the array
+// (kNoAllocScratchBytes) until the process exits; all calls share it, so
+// calls that overlap on the GPU race.  The schedule is the engine's
+// automatic one (the CTA-pair kernel above 128 reads, paced; the epilogue
+// form and the column splits the engine would pick), with the splits cut to
+// what the array holds.
 namespace r2m {
 
 constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
+constexpr size_t kNoAllocPaceBytes = kPaceSlots * sizeof(long long);
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 static __device__ __align__(256) uint32_t g_noalloc_err;
 
 static std::mutex g_noalloc_mu;
 static unsigned char *g_noalloc_ptr[64];
 static uint32_t *g_noalloc_err_ptr[64];
+static unsigned long long g_noalloc_ctx[64];  // id of the context the addresses belong to
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Process-unique id of the current context (0 when the driver cannot tell).
+static unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(p);
+  }
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // Device addresses of the scratch array and error word on the current device
-// (set up on the first call per device).
+// (looked up on the first call per device and per context).
 static int noalloc_setup(unsigned char **scratch, uint32_t **err) {
   int dev = 0;
   R2M_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(R2M_ESTATE, "device ordinal out of range");
+  const unsigned long long ctx = current_ctx_id();
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (g_noalloc_ptr[dev] == nullptr) {
+  if (g_noalloc_ptr[dev] == nullptr || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
     void *p = nullptr, *q = nullptr;
     R2M_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     R2M_CUDA(cudaGetSymbolAddress(&q, g_noalloc_err));
     g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
     g_noalloc_err_ptr[dev] = static_cast<uint32_t *>(q);
+    g_noalloc_ctx[dev] = current_ctx_id();  // the lookup made the device's context current
   }
   *scratch = g_noalloc_ptr[dev];
   *err = g_noalloc_err_ptr[dev];
@@ -1319,27 +1399,38 @@ extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_sc
   R2M_REQUIRE(score_mode != R2M_SCORE_SCALED || (reinterpret_cast<uintptr_t>(d_scaleB) & 15) == 0,
               "scaleB must be 16-byte aligned");
   const int KT = pick_kt(k);
-  const int m_tiles = (nb + BM - 1) / BM;
+  const int kind = kernel_kind(0, nb);
+  const int tile = kind == 2 ? 256 : BM;
+  const int m_tiles = (nb + tile - 1) / tile;
   const size_t list_bytes = (size_t)KT * (sizeof(float) + sizeof(int));
-  const size_t max_lists = kNoAllocScratchBytes / list_bytes;
-  if ((size_t)m_tiles * BM > max_lists)
+  const size_t max_lists = (kNoAllocScratchBytes - kNoAllocPaceBytes) / list_bytes;
+  const size_t mpad = (size_t)m_tiles * tile;
+  if (mpad > max_lists)
     return fail(R2M_EINVAL, "nb = " + std::to_string(nb) + " exceeds the allocation-free scratch (" +
                                 std::to_string(kNoAllocScratchBytes >> 20) + " MiB holds at most " +
-                                std::to_string(max_lists / BM * BM) + " rows at k = " + std::to_string(k) +
+                                std::to_string(max_lists / 256 * 256) + " rows at k = " + std::to_string(k) +
                                 "); split the batch or use r2m_batch_gemm_topk");
   unsigned char *scratch = nullptr;
   uint32_t *err = nullptr;
   int rc = noalloc_setup(&scratch, &err);
   if (rc) return rc;
   cudaStream_t st = as_stream(stream);
-  CUtensorMap mapA, mapB;
+  CUtensorMap mapA, mapB, mapB128;
   if ((rc = make_map(&mapB, d_B, N, rdim, BN))) return rc;
+  if ((rc = make_map(&mapB128, d_B, N, rdim, 128))) return rc;
   if ((rc = make_map(&mapA, d_A, nb, rdim, BM))) return rc;
   const int n_tiles = (int)((N + BN - 1) / BN);
-  const int ctas_max = sm_count();
-  int splits = choose_splits(m_tiles, n_tiles, ctas_max, 0);
-  const int fit = (int)(max_lists / ((size_t)m_tiles * BM));
-  if (splits > fit) splits = fit;
+  const int sms = sm_count();
+  const int ctas_eff = kind == 2 ? (sms / 2 > 0 ? sms / 2 : 1) : sms;
+  const int hmax = KT <= 32 ? 2 : 1;
+  // the engine's automatic schedule, with the splits cut to the scratch
+  int splits = choose_splits(m_tiles, n_tiles, ctas_eff, 0, MAX_SPLITS / hmax);
+  int halves = epi_halves_for(KT, n_tiles, splits);
+  while (splits > 1 && (size_t)halves * splits * mpad > max_lists) {
+    --splits;
+    halves = epi_halves_for(KT, n_tiles, splits);
+  }
+  if ((size_t)halves * splits * mpad > max_lists) halves = 1;
   GemmArgs g;
   g.nb = nb;
   g.num_m_tiles = m_tiles;
@@ -1348,30 +1439,56 @@ extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_sc
   g.splits = splits;
   g.num_kb = (rdim + BK - 1) / BK;
   g.score_mode = score_mode;
-  g.mpad = m_tiles * BM;
+  g.mpad = (int)mpad;
   g.scaleB = d_scaleB;
-  g.part_vals = reinterpret_cast<float *>(scratch);
-  g.part_cols = reinterpret_cast<int *>(scratch + (size_t)splits * g.mpad * KT * sizeof(float));
+  long long *pace = reinterpret_cast<long long *>(scratch);
+  unsigned char *lists = scratch + kNoAllocPaceBytes;
+  const size_t nlists = (size_t)halves * splits * mpad;
+  g.part_vals = reinterpret_cast<float *>(lists);
+  g.part_cols = reinterpret_cast<int *>(lists + nlists * KT * sizeof(float));
   g.err = err;
-  g.pace = nullptr;  // the single-CTA kernel does not pace
+  const long long units = (long long)m_tiles * splits;
+  const int ctas = (int)(units < ctas_eff ? units : ctas_eff);
+  g.pace = nullptr;
   g.pace_window = 0;
   // the error word must start at zero; the partial lists are fully
   // rewritten by the kernel before the merge reads them
   R2M_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
-  long long units = (long long)m_tiles * splits;
-  int ctas = (int)(units < ctas_max ? units : ctas_max);
-  switch (KT) {
-    case 8: rc = launch_gemm<8, 1>(mapA, mapB, g, ctas, st); break;
-    case 16: rc = launch_gemm<16, 1>(mapA, mapB, g, ctas, st); break;
-    case 20: rc = launch_gemm<20, 1>(mapA, mapB, g, ctas, st); break;
-    case 32: rc = launch_gemm<32, 1>(mapA, mapB, g, ctas, st); break;
-    default: rc = launch_gemm<64, 1>(mapA, mapB, g, ctas, st); break;
+  if (kind == 2 && ctas > 1 && ctas <= kPaceSlots) {
+    R2M_CUDA(cudaMemsetAsync(pace, 0xFF, (size_t)ctas * sizeof(long long), st));  // "not started"
+    g.pace = pace;
+    g.pace_window = PACE_WINDOW;
   }
+  rc = dispatch_gemm(kind, halves, KT, mapA, mapB, mapB128, g, ctas, st);
   if (rc) return rc;
   const int warps = 8;
-  k_merge_splits<<<(nb + warps - 1) / warps, 32 * warps, 0, st>>>(g.part_vals, g.part_cols, splits, g.mpad, KT,
-                                                                   nb, k, score_mode, d_scaleA, d_vals, d_locs);
+  k_merge_splits<<<(nb + warps - 1) / warps, 32 * warps, 0, st>>>(g.part_vals, g.part_cols, halves * splits,
+                                                                   g.mpad, KT, nb, k, score_mode, d_scaleA,
+                                                                   d_vals, d_locs);
   R2M_CUDA(cudaGetLastError());
+  k_noalloc_poison<<<64, 256, 0, st>>>(err, d_vals, d_locs, (long long)nb * k);
+  R2M_CUDA(cudaGetLastError());
+  return R2M_OK;
+}
+
+// The give-up path of the allocation-free search, driven without a fault:
+// the kernels' bounded wait, with a short limit, on an mbarrier nothing
+// arrives on, records its code in this path's error word; the poison pass
+// then marks the caller's rows as the search would.
+extern "C" int r2m_selftest_noalloc_timeout(int64_t limit_cycles, int nb, int k, float *d_vals,
+                                            int32_t *d_locs, r2m_stream_t stream) {
+  R2M_REQUIRE(limit_cycles >= 0 && limit_cycles <= (int64_t)4000000000LL, "limit_cycles must be in 0..4e9");
+  R2M_REQUIRE(nb >= 0 && k >= 1, "need nb >= 0 and k >= 1");
+  if (nb == 0) return R2M_OK;
+  R2M_REQUIRE(d_vals && d_locs, "null pointer");
+  unsigned char *scratch = nullptr;
+  uint32_t *err = nullptr;
+  int rc = noalloc_setup(&scratch, &err);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  R2M_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+  rc = launch_selftest_wait((long long)limit_cycles, 0, err, st);
+  if (rc) return rc;
   k_noalloc_poison<<<64, 256, 0, st>>>(err, d_vals, d_locs, (long long)nb * k);
   R2M_CUDA(cudaGetLastError());
   return R2M_OK;

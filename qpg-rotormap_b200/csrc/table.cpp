@@ -205,7 +205,8 @@ extern "C" int r2m_format_table(const float *vals, const int32_t *locs, int64_t 
   const size_t line_extra = 3 + 32 + 1 + 20 + 1 + max_rec + 1;
   std::vector<Buf> part((size_t)nblk);
   std::vector<size_t> used((size_t)nblk, 0);
-  std::atomic<int> bad{0};  // 1 = location out of range, 2 = record id out of range, 3 = no memory
+  std::atomic<int> bad{0};  // 1 = location out of range, 2 = record id out of range, 3 = no memory,
+                           // 4 = location -1 (rows of a search whose device wait gave up)
   auto format = [&](int64_t b) {
     const int64_t r0 = nb * b / nblk, r1 = nb * (b + 1) / nblk;
     size_t bound = 0;
@@ -226,7 +227,7 @@ extern "C" int r2m_format_table(const float *vals, const int32_t *locs, int64_t 
       for (int j = 0; j < k; ++j) {
         const int64_t c = (int64_t)locs[r * k + j] - 1;
         if (c < 0 || c >= ncols) {
-          bad = 1;
+          bad = locs[r * k + j] == -1 ? 4 : 1;
           break;
         }
         const int32_t rec = col_rec[c];
@@ -265,6 +266,9 @@ extern "C" int r2m_format_table(const float *vals, const int32_t *locs, int64_t 
   run(format);
   if (bad) {
     for (auto &b : part) give_buf(b);
+    if (bad == 4)
+      return r2m::fail(R2M_ETIMEOUT, "location -1: the search that produced this batch gave up on a "
+                                     "device-side wait (device timeout); its rows hold no result");
     if (bad == 1) return r2m::fail(R2M_EINVAL, "location out of range (1-based, 1..N)");
     if (bad == 2) return r2m::fail(R2M_EINVAL, "column record id out of range");
     return r2m::fail(R2M_ENOMEM, "table buffer allocation failed");

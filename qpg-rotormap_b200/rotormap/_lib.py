@@ -56,6 +56,7 @@ SIGNATURES = [
                                  ctypes.POINTER(I)]),
     ("r2m_batch_gemm_topk", I, [P, P, P, I, P, P, P]),
     ("r2m_batch_gemm_topk_noalloc", I, [P, P, I, I64, P, P, I, I, I, P, P, P]),
+    ("r2m_selftest_noalloc_timeout", I, [I64, I, I, P, P, P]),
     ("r2m_rescore_fp32", I, [P, I, P, I, P, P, P, I64, I, I, I, I, I, P, P, P, I, P]),
     ("r2m_check_fp64", I, [P, I, P, P, P, I64, I, I, I, I, P, I, P, P, P, P]),
     ("r2m_plain_engine_create", I, [P, I, I64, I, I, I, I, ctypes.POINTER(P)]),

@@ -13,13 +13,15 @@ kernel's read tile) into a CUDA graph and replayed; pad rows are encoded from
 zero words and their results dropped.
 
 The autotuner times the fused kernel's schedule candidates -- column splits
-around the built-in heuristic and the persistent CTA count -- on the real
-shape and keeps the fastest per (bucket, N, rdim, k).
+and persistent CTAs around the built-in heuristic, kernel, epilogue form,
+pacing window and top-k reservoir size -- on the real row count and keeps
+the fastest per (bucket, N, rdim, k, score).
 """
 from __future__ import annotations
 
 import json
 import math
+import time
 from pathlib import Path
 
 import numpy as np
@@ -33,56 +35,96 @@ def bucket_rows(n: int) -> int:
 
 
 class Autotuner:
-    """Picks (splits, ctas, epilogue) for an engine and row count by timing
-    candidates.  The epilogue form (4 or 8 warps) depends on how
-    long a work unit is, so it is only tuned when the candidates run on the
-    engine itself; on a proxy index the automatic rule stays."""
+    """Picks the fused search's schedule for an engine and a row count by
+    timing candidates on the real row count: column splits and persistent
+    CTAs (around the built-in heuristic), the kernel (single CTAs or CTA
+    pairs), the epilogue form (4 or 8 warps), the pair pacing window and the
+    top-k reservoir size -- coordinate descent from the defaults, one knob at
+    a time, each kept only when it beats the best so far.
 
-    def __init__(self, cache_path: str | None = None, reps: int = 2, proxy_cols: int = 0):
+    Cost: every candidate is one warm-up and `reps` timed searches.  When
+    that would exceed `budget` x the estimated time of one search of the
+    real shape, candidates run on a prefix of the index columns sized to fit
+    the budget (the wave behaviour -- read tiles x splits against CTAs -- is
+    the real one; work units are shorter).  Results are cached per (rows,
+    N, rdim, k, score) and, with `cache_path` (default $R2M_TUNE_CACHE),
+    kept across runs."""
+
+    RATE = 2.5e15  # FLOP/s: a model of the fused kernel, used only to size the budget
+
+    def __init__(self, cache_path: str | None = None, reps: int = 1, proxy_cols: int = 0,
+                 budget: float = 0.15, min_proxy_tiles: int = 256):
+        import os
         self.reps = reps
-        # >0: time candidates on an engine over the first proxy_cols index
-        # columns (the schedule's wave behaviour depends on read tiles x splits
-        # vs CTAs, not on the column count), then apply the winner
+        # > 0: force candidates onto the first proxy_cols index columns
         self.proxy_cols = proxy_cols
+        self.budget = budget
+        self.min_proxy_cols = 256 * min_proxy_tiles
         self.cache: dict = {}
+        cache_path = cache_path or os.environ.get("R2M_TUNE_CACHE")
         self.path = Path(cache_path) if cache_path else None
         if self.path and self.path.exists():
             self.cache = json.loads(self.path.read_text())
         self.log: list = []
+        self.last: dict = {}
 
     @staticmethod
-    def candidates(rows: int, n_cols: int, sms: int):
+    def candidates(rows: int, n_cols: int, sms: int, max_splits: int = 4):
+        """(splits, ctas) candidates: the heuristic (0) and splits around it."""
         m_tiles = (rows + 127) // 128
         n_tiles = (n_cols + 255) // 256
         smin = max(1, math.ceil(4 * sms / m_tiles))
-        cand = {0}
-        for s in (smin, 2 * smin, max(1, smin // 2), math.ceil(sms / m_tiles), math.ceil(2 * sms / m_tiles),
-                  math.ceil(8 * sms / m_tiles)):
-            if 1 <= s <= min(128, n_tiles):
-                cand.add(int(s))
-        out = [(s, 0) for s in sorted(cand)]
-        out.append((0, sms - 4 if sms > 8 else sms))
+        cand = []
+        for s in (smin, 2 * smin, max(1, smin // 2), math.ceil(2 * sms / m_tiles), math.ceil(8 * sms / m_tiles)):
+            if 1 <= s <= min(128, n_tiles) and s not in cand:
+                cand.append(int(s))
+        out = [(0, 0)] + [(s, 0) for s in sorted(cand)[:max_splits]]
+        if m_tiles < 4 * sms:  # few read tiles: fewer CTAs can balance the last wave
+            out.append((0, sms - 4 if sms > 8 else sms))
         return out
 
     def key(self, eng, rows: int) -> str:
         return f"{rows}:{eng.N}:{eng.rdim}:{eng.k}:{eng.score}"
 
+    def _proxy_cols(self, eng, rows: int, searches: int) -> int:
+        if self.proxy_cols:
+            return min(self.proxy_cols, eng.N)
+        est = 2.0 * rows * eng.N * eng.rdim / self.RATE
+        per = self.budget * est / max(searches, 1)
+        cols = int(per * self.RATE / (2.0 * rows * eng.rdim))
+        cols = max(cols, self.min_proxy_cols)
+        return eng.N if cols >= eng.N else cols // 256 * 256
+
+    @staticmethod
+    def _apply(eng, cfg):
+        eng.set_tuning(cfg["splits"], cfg["ctas"], kernel=cfg["kernel"], epilogue=cfg["epilogue"],
+                       pace=cfg["pace"], kt=cfg["kt"])
+
     def tune(self, eng, A8: torch.Tensor, rows: int, scaleA=None, stream=None):
         k = self.key(eng, rows)
         if k in self.cache:
-            s, c, *rest = self.cache[k]
-            ep = rest[0] if rest else "auto"
-            eng.set_tuning(s, c, epilogue=ep)
-            return s, c
+            cfg = self.cache[k]
+            if isinstance(cfg, list):  # older cache entries: (splits, ctas[, epilogue])
+                cfg = {"splits": cfg[0], "ctas": cfg[1], "kernel": "auto",
+                       "epilogue": cfg[2] if len(cfg) > 2 else "auto", "pace": 0, "kt": 0}
+            self._apply(eng, cfg)
+            self.last = dict(cfg, cached=True)
+            return cfg["splits"], cfg["ctas"]
         sms = torch.cuda.get_device_properties(eng.device).multi_processor_count
         st = stream or torch.cuda.current_stream(eng.device)
+        split_c = self.candidates(rows, eng.N, sms)
+        kt_c = [0] + ([32] if eng.k <= 20 else [64] if eng.k <= 32 else [])
+        n_trials = len(split_c) + 1 + (2 if eng.k <= 32 else 0) + 2 + len(kt_c) - 1
+        cols = self._proxy_cols(eng, rows, n_trials * (1 + self.reps))
         target = eng
-        if 0 < self.proxy_cols < eng.N:
+        if cols < eng.N:
             from .engine import TopKEngine
-            sb = eng.scaleB[:self.proxy_cols] if eng.scaleB is not None else None
-            target = TopKEngine(eng.B[:self.proxy_cols], k=eng.k, rows_cap=eng.rows_cap, score=eng.score, scaleB=sb)
-        def timed(s, c, ep):
-            target.set_tuning(s, c, epilogue=ep)
+            sb = eng.scaleB[:cols] if eng.scaleB is not None else None
+            target = TopKEngine(eng.B[:cols], k=eng.k, rows_cap=eng.rows_cap, score=eng.score, scaleB=sb)
+        t_start = time.perf_counter()
+
+        def timed(cfg):
+            self._apply(target, cfg)
             target.search(A8, rows, scaleA, stream=st)  # warm
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
@@ -91,26 +133,41 @@ class Autotuner:
             e1.record(st)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / self.reps
-            self.log.append({"rows": rows, "splits": s, "ctas": c, "epilogue": ep, "ms": ms})
+            self.log.append(dict(cfg, rows=rows, cols=cols, ms=ms))
             return ms
 
-        best, best_ms = (0, 0, "auto"), float("inf")
-        for s, c in self.candidates(rows, eng.N, sms):
-            ms = timed(s, c, "auto")
+        best = {"splits": 0, "ctas": 0, "kernel": "auto", "epilogue": "auto", "pace": 0, "kt": 0}
+        default_ms = best_ms = timed(best)
+
+        def consider(**change):
+            nonlocal best, best_ms
+            cfg = dict(best, **change)
+            if cfg == best:
+                return
+            ms = timed(cfg)
             if ms < best_ms:
-                best, best_ms = (s, c, "auto"), ms
-        if target is eng and eng.k <= 32:  # the fused kernels' two epilogue forms
-            for ep in ("4", "8"):
-                ms = timed(best[0], best[1], ep)
-                if ms < best_ms:
-                    best, best_ms = (best[0], best[1], ep), ms
+                best, best_ms = cfg, ms
+
+        for s, c in split_c[1:]:
+            consider(splits=s, ctas=c)
+        consider(kernel="1sm" if rows > 128 else "2sm")
+        if eng.k <= 32:
+            consider(epilogue="4")
+            consider(epilogue="8")
+        consider(pace=32)
+        consider(pace=-1)
+        for kt in kt_c[1:]:
+            consider(kt=kt)
         if target is not eng:
             target.close()
-        eng.set_tuning(best[0], best[1], epilogue=best[2])
-        self.cache[k] = list(best)
+        self._apply(eng, best)
+        self.last = dict(best, ms=best_ms, default_ms=default_ms, proxy_cols=cols,
+                         tune_s=time.perf_counter() - t_start, cached=False)
+        self.cache[k] = best
         if self.path:
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.path.write_text(json.dumps(self.cache))
-        return best[0], best[1]
+        return best["splits"], best["ctas"]
 
 
 class RaggedBatcher:
@@ -157,7 +214,10 @@ class RaggedBatcher:
             if self.tuner is not None:
                 sa = self.eng.scaleA[:rows] if self.eng.score == "scaled" else None
                 self.tuner.tune(self.eng, self.eng.a8, rows, sa, self.stream)
-            self._step(rows)  # eager warm-up (first calls set kernel attributes)
+            # eager warm-up on one read tile: the step's first calls load the
+            # encoder and set its launch attributes outside the capture (the
+            # engine loads its fused kernels when it is created)
+            self._step(min(rows, 128))
         self.stream.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):

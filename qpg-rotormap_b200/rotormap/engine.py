@@ -59,7 +59,7 @@ class TopKEngine:
     def __init__(self, B: torch.Tensor, k: int = 20, w: int | None = None, rows_cap: int = 8192,
                  segs: int | None = None, score: str = "f16", scaleB: torch.Tensor | None = None,
                  splits: int = 0, ctas: int = 0, timing: bool = False, kernel: str = "auto",
-                 epilogue: str = "auto", pace: int = 0):
+                 epilogue: str = "auto", pace: int = 0, kt: int = 0):
         _lib.require_device()
         if B.dtype != torch.uint8 or B.dim() != 2 or not B.is_cuda or not B.is_contiguous():
             raise ValueError("B must be a contiguous (N, rdim) uint8 CUDA tensor")
@@ -84,7 +84,8 @@ class TopKEngine:
         tune.reserved[1] = _KERNELS[kernel]
         tune.reserved[2] = _EPILOGUES[epilogue]
         tune.reserved[3] = int(pace)
-        self.kernel, self.epilogue, self.pace = kernel, epilogue, int(pace)
+        tune.reserved[4] = int(kt)
+        self.kernel, self.epilogue, self.pace, self.kt = kernel, epilogue, int(pace), int(kt)
         h = ctypes.c_void_p()
         check(lib().r2m_engine_create(ptr(B), ptr(scaleB), rdim, N, k, rows_cap, _MODES[score],
                                       ctypes.byref(tune), ctypes.byref(h)))
@@ -95,20 +96,26 @@ class TopKEngine:
         return self.B.device
 
     def set_tuning(self, splits: int = 0, ctas: int = 0, kernel: str | None = None,
-                   epilogue: str | None = None, pace: int | None = None) -> None:
+                   epilogue: str | None = None, pace: int | None = None, kt: int | None = None) -> None:
         """Change the schedule (0 = automatic; pace: 0 default pacing window,
-        > 0 window in column tiles, < 0 off).  Not during stream capture."""
+        > 0 window in column tiles, < 0 off; kt: top-k reservoir size, 0 auto,
+        else 8/16/20/32/64 >= k).  Not during stream capture."""
         kernel = kernel or self.kernel
         epilogue = epilogue or self.epilogue
         pace = self.pace if pace is None else int(pace)
+        kt = self.kt if kt is None else int(kt)
         if epilogue not in _EPILOGUES:
             raise ValueError("epilogue must be 'auto', '4' or '8'")
+        if kernel not in _KERNELS:
+            raise ValueError("kernel must be 'auto', '1sm' or '2sm'")
         t = Tuning(splits, ctas)
         t.reserved[1] = _KERNELS[kernel]
         t.reserved[2] = _EPILOGUES[epilogue]
         t.reserved[3] = pace
+        t.reserved[4] = kt
         check(lib().r2m_engine_set_tuning(self._h, ctypes.byref(t)))
-        self.splits, self.ctas, self.kernel, self.epilogue, self.pace = splits, ctas, kernel, epilogue, pace
+        self.splits, self.ctas, self.kernel, self.epilogue, self.pace, self.kt = (splits, ctas, kernel, epilogue,
+                                                                                  pace, kt)
 
     def kernel_ms(self):
         """(gemm_ms, merge_ms, splits) of the last search (timing engines only)."""

@@ -65,9 +65,35 @@ def test_autotuner_keeps_results(setup, tmp_path):
     tuner = rm.Autotuner(str(tmp_path / "tune.json"))
     b = rm.RaggedBatcher(eng, re, total, tuner=tuner, use_graphs=True)
     got = b.run(sub)
-    assert len(tuner.log) >= 3 and (tmp_path / "tune.json").exists()
-    eng.set_tuning(0, 0)
+    assert len(tuner.log) >= 6 and (tmp_path / "tune.json").exists()
+    assert {"kernel", "epilogue", "pace", "kt"} <= set(tuner.log[0])
+    eng.set_tuning(0, 0, kernel="auto", epilogue="auto", pace=0, kt=0)
     ref = _per_request(eng, re, sub)
     for (v, l), (rv, rl) in zip(got, ref):
         assert np.array_equal(v, rv) and np.array_equal(l, rl)
+    # a second tuner reads the persisted choice instead of timing again
+    t2 = rm.Autotuner(str(tmp_path / "tune.json"))
+    b2 = rm.RaggedBatcher(eng, re, total, tuner=t2, use_graphs=True)
+    got2 = b2.run(sub)
+    assert t2.log == [] and t2.last.get("cached")
+    for (v, l), (rv, rl) in zip(got2, ref):
+        assert np.array_equal(v, rv) and np.array_equal(l, rl)
+    eng.close()
+
+
+@pytest.mark.parametrize("cfg", [dict(kernel="1sm"), dict(kernel="2sm"), dict(epilogue="4"), dict(epilogue="8"),
+                                 dict(pace=32), dict(pace=-1), dict(kt=32), dict(kt=64), dict(splits=3),
+                                 dict(ctas=100)])
+def test_every_schedule_gives_identical_results(setup, cfg):
+    """The autotuner may pick any of these: none may change a result."""
+    re, idx, reqs = setup
+    w = np.concatenate(reqs[:6])
+    d = torch.from_numpy(w.reshape(-1).view(np.int32)).cuda()
+    a8, _ = rm.encode_frag_real_batch_alloc(torch.uint8, re, d)
+    eng = rm.TopKEngine(idx.embeds8, k=20, rows_cap=a8.shape[0])
+    v0, l0 = (t.cpu().numpy() for t in eng.search(a8))
+    eng.set_tuning(cfg.get("splits", 0), cfg.get("ctas", 0), kernel=cfg.get("kernel"),
+                   epilogue=cfg.get("epilogue"), pace=cfg.get("pace"), kt=cfg.get("kt"))
+    v1, l1 = (t.cpu().numpy() for t in eng.search(a8))
+    assert np.array_equal(v0, v1) and np.array_equal(l0, l1)
     eng.close()

@@ -10,7 +10,9 @@ import numpy as np
 import pytest
 
 import rotormap as rm
+import torch
 from rotormap import serving, synth
+from topk_check import assert_topk_rows, oracle_scores_at
 
 pytestmark = pytest.mark.gpu
 
@@ -30,6 +32,13 @@ def setup():
         reads, hd, _, _ = synth.sample_reads_even(heads, recs, n, K, float(rng.uniform(0, 0.1)), seed=100 + i)
         reqs.append(synth.pack_reads(reads, K))
     return re, idx, reqs
+
+
+def _encode_host(re, words):
+    """The e4m3 rows the server searches with (the library's encoder)."""
+    dw = torch.from_numpy(np.ascontiguousarray(words).reshape(-1).view(np.int32)).cuda()
+    a8, _ = rm.encode_frag_real_batch_alloc(torch.uint8, re, dw)
+    return a8.cpu().numpy()
 
 
 def _serve(eng, re, reqs, budget=None, stagger=0.0):
@@ -95,10 +104,11 @@ def test_served_results_match_plain_path(setup):
     # the reference-structured engine (cuBLASLt + segmented top-k)
     peng = rm.PlainEngine(idx.embeds8, k=20, w=65536, rows_cap=8192)
     ref = serving.plain_map(peng, re, [(0.0, w) for w in reqs], batch=8192)
-    overlap = []
-    for (v, l), (_, pv, pl) in zip(mix, ref):
-        np.testing.assert_allclose(v, pv, rtol=0, atol=1e-3)
-        overlap += [len(set(a) & set(b)) / 20 for a, b in zip(l, pl)]
-    assert np.mean(overlap) > 0.97
+    # the reference-structured engine keeps an arbitrary one of tied
+    # locations; every location that differs is a tie within one fp16 step
+    B = idx.embeds8.cpu().numpy()
+    for w, (v, l), (_, pv, pl) in zip(reqs, mix, ref):
+        a8 = _encode_host(re, w)
+        assert_topk_rows(v, l, pv, pl, oracle_scores_at(a8, B, l, 0), tol=1e-3, N=idx.N)
     peng.close()
     eng.close()
