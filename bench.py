@@ -260,9 +260,12 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31):
         wait(a)
         hs.append(srv.submit(w, t_arrival=t0 + a))
     res = [h.result(600) for h in hs]
+    done_times = [h.t_done for h in hs]  # results in host memory (CLOCK_MONOTONIC = perf_counter's clock)
+    sst = srv.stats()
     srv.close()
-    out["serving"] = stats([h.t_done for h in hs], t0)
-    out["serving"]["batches"] = srv.batches
+    out["serving"] = stats(done_times, t0)
+    out["serving"]["batches"] = sst.batches
+    out["serving"]["loop"] = "native (r2m_server_*)"
     out["serving"]["tflops"] = total * flop_per_read / out["serving"]["span_s"] / 1e12
     # plain batch path, reference engine structure (cuBLASLt fp8 + segmented top-k, batch 8192)
     peng = rm.PlainEngine(idx.embeds8, k=TOPK, w=65536, rows_cap=8192)

@@ -161,6 +161,10 @@ int r2m_engine_destroy(r2m_engine *eng);
  * it outside stream capture).  No reference counterpart (the reference's
  * schedule knobs are the constructor's w / segs). */
 int r2m_engine_set_tuning(r2m_engine *eng, const r2m_tuning *tune);
+/* The engine's top-k size, row width, score mode, batch height and column
+ * count (any pointer may be NULL).  No reference counterpart (the reference
+ * reads these from the TopKEngine struct's fields). */
+int r2m_engine_info(const r2m_engine *eng, int *k, int *rdim, int *score_mode, int *rows_cap, int64_t *N);
 /* Bytes of device workspace the engine holds. */
 int64_t r2m_engine_workspace_bytes(const r2m_engine *eng);
 /* Device time of the last r2m_batch_gemm_topk's GEMM+top-k kernel and of
@@ -399,6 +403,77 @@ const int64_t *r2m_dreads_spans(const r2m_dreads *r);
 /* device, every kept header followed by one '\n' (total bytes in *total_len) */
 const uint8_t *r2m_dreads_header_blob(const r2m_dreads *r, size_t *total_len);
 void r2m_dreads_free(r2m_dreads *r);
+
+/* ---------------------------------------------------------- serving form */
+
+/* The serving form: a continuous-batching request loop over one fused
+ * engine, on the library's own streams and one loop thread.  It replaces the
+ * per-file driver loop of run_map (RotorMap/tools/map.jl:100-184, which maps
+ * one read file at a time through rope_topk_stream_compact in synchronous
+ * batches) for hosts that map many requests at once: requests of any size
+ * arrive from any thread; each is admitted, in arrival order, when its
+ * device state (words + result lists, r2m_server_request_bytes) fits both
+ * the byte budget and the device memory free at that moment less
+ * `hbm_reserve`; every GPU batch is cut from all admitted requests (a
+ * request that arrives while others run joins the next batch).  A read's
+ * result does not depend on the batch it lands in.  Cancelling a queued
+ * request drops it; cancelling an admitted one stops its remaining rows and
+ * frees it once its rows in flight are done, leaving other requests
+ * untouched.  A failed CUDA call fails every unfinished request with that
+ * first error and closes the server (first error wins, as the reference's
+ * err_out, RotorMap/encode/stream.jl:95-110). */
+typedef struct r2m_server r2m_server;
+
+enum { R2M_REQ_QUEUED = 0, R2M_REQ_ACTIVE = 1, R2M_REQ_DONE = 2, R2M_REQ_CANCELLED = 3, R2M_REQ_FAILED = 4 };
+
+typedef struct {
+  int64_t batches, rows, max_rows;          /* GPU batches launched, rows in them, tallest */
+  int64_t requests_done, requests_cancelled, requests_failed;
+  int64_t in_use_bytes, peak_in_use_bytes;  /* admitted requests' device state */
+  int64_t queued, active;                   /* requests waiting / admitted now */
+} r2m_server_stats;
+
+/* eng: a fused engine (its rows_cap is the batch height, its score mode the
+ * quantisation: scaled e4m3 rows for R2M_SCORE_SCALED, else the reference's
+ * e4m3); (k, s, m, c, normalize): the encoder, matching the engine's row
+ * width.  hbm_budget 0 = no byte budget (free memory alone); max_inflight:
+ * GPU batches queued ahead (0 = 2).  The engine must outlive the server and
+ * must not be used by others meanwhile. */
+int r2m_server_create(r2m_engine *eng, int k, int s, int m, int c, int normalize, int64_t hbm_budget,
+                      int64_t hbm_reserve, int max_inflight, r2m_server **out);
+/* Submit n reads (h_words: n * cld(k,16) forward 2-bit words).  Results go
+ * to the caller's h_vals / h_locs (n, k) when the request is done; all three
+ * buffers must stay valid until then (page-locked buffers are copied
+ * asynchronously, pageable ones synchronously by the loop thread).
+ * t_arrival: CLOCK_MONOTONIC seconds of the arrival (<= 0: now).  A request
+ * larger than the byte budget returns R2M_ENOMEM. */
+int r2m_server_submit(r2m_server *srv, const uint32_t *h_words, int64_t n, float *h_vals, int32_t *h_locs,
+                      double t_arrival, int64_t *id);
+/* Submit FASTA bytes (parsed now by r2m_fasta_reads with the reference's
+ * trim / skip rules; the reads' headers: r2m_server_reads).  Input that does
+ * not start with a '>' header, or keeps no read of k bases, returns R2M_EIO.
+ * Results: r2m_server_copy_result. */
+int r2m_server_submit_fasta(r2m_server *srv, const char *data, size_t len, int nthreads, double t_arrival,
+                            int64_t *id, int64_t *n_reads);
+int r2m_server_cancel(r2m_server *srv, int64_t id);
+/* Block until the request has finished (timeout_s < 0: no limit; R2M_ETIMEOUT
+ * when it runs out); *state = its R2M_REQ_* state. */
+int r2m_server_wait(r2m_server *srv, int64_t id, double timeout_s, int *state);
+/* State, read count and CLOCK_MONOTONIC times of a request. */
+int r2m_server_request(r2m_server *srv, int64_t id, int *state, int64_t *n, double *t_arrival,
+                       double *t_admit, double *t_done);
+const char *r2m_server_request_error(r2m_server *srv, int64_t id);
+/* Copy a done request's results (needed for FASTA requests; a no-op copy
+ * for the caller's own buffers). */
+int r2m_server_copy_result(r2m_server *srv, int64_t id, float *h_vals, int32_t *h_locs);
+const r2m_reads *r2m_server_reads(r2m_server *srv, int64_t id);
+/* Forget a finished request (its id becomes unknown). */
+int r2m_server_release(r2m_server *srv, int64_t id);
+int r2m_server_get_stats(r2m_server *srv, r2m_server_stats *out);
+int64_t r2m_server_request_bytes(const r2m_server *srv, int64_t n);
+/* Stop the loop: finish every request first (cancel_pending = 0) or cancel
+ * the unfinished ones; frees the server.  Returns the first loop failure. */
+int r2m_server_destroy(r2m_server *srv, int cancel_pending);
 
 /* ------------------------------------------- reference index file (.bin) */
 

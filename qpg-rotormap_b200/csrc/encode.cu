@@ -25,6 +25,8 @@
 // 32-window batch; the group's leader adds them in lane order).  The output
 // conversion (fp32 / fp16 / e4m3 / scaled e4m3) is fused into the final pass.
 #include <math.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include "common.cuh"
 
@@ -43,6 +45,7 @@ struct EncParams {
   int hist_floats;  // per-warp histogram floats (2*nbin, rounded to whole 16-bin chunks)
   int cs_u16;       // per-warp csmer slots (nw rounded up to 8)
   int words_u32;    // per-warp staged words (W + 2, rounded up to 4)
+  int sp_nslot;     // sparse path: most distinct c-mers a fragment can have, min(nw, 4^c)
 };
 
 static int make_params(EncParams &P, int k, int s, int m, int c, int normalize) {
@@ -74,6 +77,10 @@ static int make_params(EncParams &P, int k, int s, int m, int c, int normalize) 
   P.hist_floats = (P.rdim + 31) & ~31;
   P.cs_u16 = (P.nw + 7) & ~7;
   P.words_u32 = (P.W + 2 + 3) & ~3;
+  {
+    const long long ncm = 1LL << (2 * c);
+    P.sp_nslot = (int)(ncm < P.nw ? ncm : P.nw);
+  }
   return R2M_OK;
 }
 
@@ -640,6 +647,364 @@ __global__ void k_revcomp(uint32_t *drc, const uint32_t *dnas, int W, int64_t n,
   drc[g] = lanerev32(v);
 }
 
+// ------------------------------------------------------------------
+// Sparse fragment encoder (normalize = 0).
+//
+// At read length a fragment has few windows (143 at k = 150) against many
+// bins (1024 complex bins at s8 m4 c4), so a dense per-warp histogram is
+// mostly zeros that are cleared, summed and scanned again.  This path keeps
+// one accumulator of m complex bins per DISTINCT c-mer of the fragment (a
+// slot; slots are numbered in order of first appearance and a 4^c-byte map
+// gives each c-mer's slot).  Windows are added in increasing window order:
+// within a 32-window batch the members of a c-mer group add in rounds, by
+// their rank in the group, so every bin is the same sum, formed in the same
+// order, as the dense histogram's.  The norm and the row maximum are taken
+// over the slots; each slot's values are divided, scaled and converted once;
+// the output pass writes the dense row in 16-byte chunks, c-mer-major, with
+// each c-mer's converted values taken from its slot, or zero.  The words of
+// the fragment live in registers (lane t holds word t) and every window's
+// 2s-bit field comes from two shuffles; the reverse complement of an index
+// window is formed the same way.
+
+template <int N>
+struct Bytes;
+template <>
+struct Bytes<1> { using T = uint8_t; };
+template <>
+struct Bytes<2> { using T = uint16_t; };
+template <>
+struct Bytes<4> { using T = uint32_t; };
+template <>
+struct Bytes<8> { using T = uint2; };
+template <>
+struct Bytes<16> { using T = uint4; };
+
+__device__ __forceinline__ unsigned long long f2_bits(float2 a) {
+  return *reinterpret_cast<const unsigned long long *>(&a);
+}
+__device__ __forceinline__ float2 bits_f2(unsigned long long x) { return *reinterpret_cast<const float2 *>(&x); }
+// Paired fp32 arithmetic (sm_100 f32x2): each half is the IEEE result of
+// the scalar operation.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(d);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return bits_f2(d);
+}
+
+// m values of one part (Re or Im) of a c-mer -> their m * bytes(OUT)
+// output bytes, in the row's element order.
+template <int OUT, int M>
+__device__ __forceinline__ typename Bytes<M * OutT<OUT>::bytes>::T pack_part(const float (&v)[M]) {
+  constexpr int CB = M * OutT<OUT>::bytes;
+  union {
+    typename Bytes<CB>::T t;
+    uint32_t w[(CB + 3) / 4];
+    uint16_t h[(CB + 1) / 2];
+    uint8_t b[CB];
+  } u;
+  if constexpr (OUT == R2M_OUT_F32) {
+#pragma unroll
+    for (int q = 0; q < M; ++q) u.w[q] = __float_as_uint(v[q]);
+  } else if constexpr (OUT == R2M_OUT_F16) {
+    if constexpr (M == 1) {
+      u.h[0] = __half_as_ushort(__float2half_rn(v[0]));
+    } else {
+#pragma unroll
+      for (int q = 0; q < M / 2; ++q) {
+        __half2 t = __floats2half2_rn(v[2 * q], v[2 * q + 1]);
+        u.w[q] = *reinterpret_cast<uint32_t *>(&t);
+      }
+    }
+  } else {
+    // e4m3 pairs: low byte = first value
+    uint16_t pr[(M + 1) / 2];
+#pragma unroll
+    for (int q = 0; q < (M + 1) / 2; ++q) {
+      const float a = v[2 * q], b = (2 * q + 1 < M) ? v[2 * q + 1] : 0.0f;
+      if constexpr (OUT == R2M_OUT_E4M3) {
+        __half2 h = __floats2half2_rn(a, b);
+        asm("cvt.rn.satfinite.e4m3x2.f16x2 %0, %1;" : "=h"(pr[q]) : "r"(*reinterpret_cast<uint32_t *>(&h)));
+      } else {
+        pr[q] = f32x2_to_e4m3x2(a, b);
+      }
+    }
+    if constexpr (M == 1) {
+      u.b[0] = (uint8_t)(pr[0] & 0xFF);
+    } else {
+#pragma unroll
+      for (int q = 0; q < M / 2; ++q) u.h[q] = pr[q];
+    }
+  }
+  return u.t;
+}
+
+// Per-warp shared memory of the sparse path (sizes in SparseLayout).
+struct SparseLayout {
+  int smap, acc, conv;  // byte sizes: slot map, accumulators, one conversion array
+  int warp;             // total per warp
+};
+
+__host__ __device__ inline SparseLayout sparse_layout(int c, int m, int nslot, int outb) {
+  SparseLayout L;
+  const int ncm = 1 << (2 * c);
+  L.smap = (ncm + 15) & ~15;
+  L.acc = ((nslot * m * 8) + 15) & ~15;
+  L.conv = ((nslot * m * outb) + 15) & ~15;
+  L.warp = L.smap + L.acc + 2 * L.conv;
+  return L;
+}
+
+// Encode the fragment whose W words are in `wreg` (lane t: word t, zero for
+// t >= W) with one warp into `row`, its m norms and (scaled) its row scale.
+template <int OUT, int M>
+__device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2 *__restrict__ table,
+                                                unsigned char *warea, uint32_t wreg, unsigned char *row,
+                                                float *norms_out, float *scale_out) {
+  constexpr int OUTB = OutT<OUT>::bytes, CB = M * OUTB, CPC = 16 / CB;
+  using T = typename Bytes<CB>::T;
+  using TM = typename Bytes<CPC>::T;
+  const SparseLayout L = sparse_layout(P.c, M, P.sp_nslot, OUTB);
+  uint8_t *smap = warea;
+  float2 *acc = reinterpret_cast<float2 *>(warea + L.smap);
+  T *conv_re = reinterpret_cast<T *>(warea + L.smap + L.acc);
+  T *conv_im = reinterpret_cast<T *>(warea + L.smap + L.acc + L.conv);
+  const int lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+  const unsigned lt = (1u << lane) - 1u;
+  const int ncm = 1 << (2 * P.c);
+  for (int i = lane * 16; i < ncm; i += 512) *reinterpret_cast<uint4 *>(smap + i) = make_uint4(~0u, ~0u, ~0u, ~0u);
+  __syncwarp();
+  // ---- accumulate, window order
+  int nslots = 0;
+  for (int b0 = 0; b0 < P.nw; b0 += 32) {
+    const int p = b0 + lane;
+    const bool valid = p < P.nw;
+    const int wo = p >> 4;
+    const uint32_t w0 = __shfl_sync(FULL, wreg, wo & 31), w1 = __shfl_sync(FULL, wreg, (wo + 1) & 31);
+    const uint32_t v = __funnelshift_r(w0, w1, (uint32_t)(p & 15) << 1);
+    const uint32_t smer = v & P.bmask;
+    const uint32_t upper = (2 * P.c >= 32) ? 0u : (smer >> (2 * P.c));
+    const uint32_t cb = (smer & P.cbmask) ^ ((upper * 0x9E3779B1u) & P.cbmask);
+    const unsigned grp = __match_any_sync(FULL, valid ? cb : (0x40000000u | (uint32_t)lane));
+    const int rank = __popc(grp & lt);
+    const bool leader = valid && rank == 0;
+    int s_l = 0xFF;
+    if (leader) s_l = smap[cb];
+    const bool isnew = leader && s_l == 0xFF;
+    const unsigned newm = __ballot_sync(FULL, isnew);
+    if (isnew) {
+      s_l = nslots + __popc(newm & lt);
+      smap[cb] = (uint8_t)s_l;
+    }
+    nslots += __popc(newm);
+    const int slot = __shfl_sync(FULL, s_l, __ffs(grp) - 1);
+    float2 ph[M];
+    if (valid) {
+      if constexpr (M == 1) {
+        ph[0] = table[p];
+      } else {
+        const float4 *t4 = reinterpret_cast<const float4 *>(table + (size_t)p * M);
+#pragma unroll
+        for (int q = 0; q < M / 2; ++q) {
+          const float4 t = t4[q];
+          ph[2 * q] = make_float2(t.x, t.y);
+          ph[2 * q + 1] = make_float2(t.z, t.w);
+        }
+      }
+    }
+    const int rounds = (int)__reduce_max_sync(FULL, valid ? (unsigned)rank : 0u);
+    for (int r = 0; r <= rounds; ++r) {
+      if (valid && rank == r) {
+        float2 *a = acc + (size_t)slot * M;
+        if (r == 0 && isnew) {
+          const float2 z = make_float2(0.f, 0.f);  // 0 + x, as a cleared histogram bin
+#pragma unroll
+          for (int q = 0; q < M; ++q) a[q] = add2(z, ph[q]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < M; ++q) a[q] = add2(a[q], ph[q]);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // ---- the G-homopolymer c-mer's bins are zero
+  if (lane == 0) {
+    const int sg = smap[P.csmerG];
+    if (sg != 0xFF) {
+#pragma unroll
+      for (int q = 0; q < M; ++q) acc[(size_t)sg * M + q] = make_float2(0.f, 0.f);
+    }
+  }
+  __syncwarp();
+  // ---- per-copy energies and the largest magnitude
+  float part[M], mx = 0.f;
+#pragma unroll
+  for (int q = 0; q < M; ++q) part[q] = 0.f;
+  for (int sl = lane; sl < nslots; sl += 32) {
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const float2 z = acc[(size_t)sl * M + q];
+      part[q] += __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
+      mx = fmaxf(mx, fmaxf(fabsf(z.x), fabsf(z.y)));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < M; ++q) part[q] += __shfl_xor_sync(FULL, part[q], o);
+    mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+  }
+  float tot = part[0];
+#pragma unroll
+  for (int q = 1; q < M; ++q) tot += part[q];
+  const float nrm = (float)((double)sqrtf(tot) + 1e-16);
+#pragma unroll
+  for (int q = 0; q < M; ++q)
+    if (lane == q) norms_out[q] = q == 0 ? nrm : part[q];
+  // x / nrm for every value with one reciprocal: y = RN(1/nrm), q0 = x*y,
+  // r = x - q0*nrm (exact with FMA), RN(q0 + r*y) is the correctly rounded
+  // quotient (Markstein) -- the reference's fp32 `hist ./= nrm`
+  const float y = __frcp_rn(nrm);
+  const float2 y2 = make_float2(y, y), nn2 = make_float2(-nrm, -nrm);
+  float scale = 1.0f;
+  if constexpr (OUT == R2M_OUT_E4M3_SCALED) {
+    const float q0 = mx * y;
+    const float amax = fmaf(fmaf(-q0, nrm, mx), y, q0);
+    scale = amax > 0.f ? 448.0f / amax : 1.0f;
+    if (lane == 0) *scale_out = amax > 0.f ? amax / 448.0f : 0.0f;
+  }
+  const float2 sc2 = make_float2(scale, scale);
+  // ---- convert each slot once
+  for (int sl = lane; sl < nslots; sl += 32) {
+    float re[M], im[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const float2 x = acc[(size_t)sl * M + q];
+      const float2 q0 = mul2(x, y2);
+      float2 d = fma2(fma2(q0, nn2, x), y2, q0);
+      if constexpr (OUT == R2M_OUT_E4M3_SCALED) d = mul2(d, sc2);
+      re[q] = d.x;
+      im[q] = d.y;
+    }
+    conv_re[sl] = pack_part<OUT, M>(re);
+    conv_im[sl] = pack_part<OUT, M>(im);
+  }
+  __syncwarp();
+  // ---- the dense row, 16-byte chunks, c-mer-major: [Re part | Im part]
+  const int nch = (ncm * CB) >> 4;  // chunks per part
+  for (int j = lane; j < 2 * nch; j += 32) {
+    const bool isim = j >= nch;
+    const int jj = isim ? j - nch : j;
+    union {
+      TM t;
+      uint8_t b[CPC];
+    } sm;
+    sm.t = *reinterpret_cast<const TM *>(smap + jj * CPC);
+    const T *cv = isim ? conv_im : conv_re;
+    union {
+      uint4 v;
+      T t[CPC];
+    } o;
+#pragma unroll
+    for (int e = 0; e < CPC; ++e) {
+      T val = T();
+      const int sl = sm.b[e];
+      if (sl != 0xFF) val = cv[sl];
+      o.t[e] = val;
+    }
+    *reinterpret_cast<uint4 *>(row + (isim ? ncm * CB : 0) + ((size_t)jj << 4)) = o.v;
+  }
+  __syncwarp();
+}
+
+// Phasor table of the sparse path: entry p * m + idm (the m copies of a
+// window side by side), the reference thread's exact fp32 values.
+__device__ __forceinline__ void sparse_table(const EncParams &P, float2 *t) {
+  const int total = P.m * P.nw;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) t[i] = ref_phasor(P, i % P.m, i / P.m);
+  __syncthreads();
+}
+
+__host__ __device__ inline size_t sparse_table_bytes(const EncParams &P) {
+  return ((size_t)P.m * P.nw * 8 + 15) & ~(size_t)15;
+}
+
+template <int OUT, int M>
+__global__ void __launch_bounds__(256) k_encode_sparse(EncParams P, const uint32_t *__restrict__ dnas, int64_t n,
+                                                       void *dest, float *norms, float *scales) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2 *table = reinterpret_cast<float2 *>(smem);
+  sparse_table(P, table);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const SparseLayout L = sparse_layout(P.c, M, P.sp_nslot, OutT<OUT>::bytes);
+  unsigned char *warea = smem + sparse_table_bytes(P) + (size_t)L.warp * warp;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const size_t rowbytes = (size_t)P.rdim * OutT<OUT>::bytes;
+  int64_t f = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  uint32_t wnext = (f < n && lane < P.W) ? __ldg(dnas + f * P.W + lane) : 0u;
+  for (; f < n; f += nwarps) {
+    const uint32_t wreg = wnext;
+    const int64_t fn = f + nwarps;
+    wnext = (fn < n && lane < P.W) ? __ldg(dnas + fn * P.W + lane) : 0u;  // next fragment's words in flight
+    sparse_fragment<OUT, M>(P, table, warea, wreg, reinterpret_cast<unsigned char *>(dest) + rowbytes * f,
+                            norms + f * M, scales ? scales + f : nullptr);
+  }
+}
+
+template <int OUT, int M>
+__global__ void __launch_bounds__(256) k_encode_sparse_ref(EncParams P, const uint32_t *__restrict__ genome,
+                                                           const int64_t *__restrict__ win_pos, int64_t nwin,
+                                                           int64_t batch, void *dest, float *norms,
+                                                           float *scales) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2 *table = reinterpret_cast<float2 *>(smem);
+  sparse_table(P, table);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned FULL = 0xFFFFFFFFu;
+  const SparseLayout L = sparse_layout(P.c, M, P.sp_nslot, OutT<OUT>::bytes);
+  unsigned char *warea = smem + sparse_table_bytes(P) + (size_t)L.warp * warp;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const size_t rowbytes = (size_t)P.rdim * OutT<OUT>::bytes;
+  const int rr = P.k & 15;
+  const uint32_t tailmask = rr == 0 ? 0xFFFFFFFFu : ((1u << (2 * rr)) - 1u);
+  const uint32_t shbits = (uint32_t)(32 * P.W - 2 * P.k);
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; i < nwin; i += nwarps) {
+    const int64_t pos = __ldg(win_pos + i);
+    const int64_t q = pos >> 4;
+    uint32_t fw = 0u;
+    if (lane < P.W) {
+      const uint32_t a = __ldg(genome + q + lane), b = __ldg(genome + q + lane + 1);
+      fw = __funnelshift_r(a, b, (uint32_t)(pos & 15) << 1);
+      if (lane == P.W - 1) fw &= tailmask;
+    }
+    // reverse complement: complement, left-align the k bases to the end of
+    // the W-word stream, reverse the word order and the sixteen 2-bit lanes
+    const int src = P.W - 1 - lane;
+    const uint32_t xi = ~__shfl_sync(FULL, fw, src & 31), xm = ~__shfl_sync(FULL, fw, (src - 1) & 31);
+    uint32_t vv = xi;
+    if (shbits != 0) vv = (xi << shbits) | (src > 0 ? (xm >> (32u - shbits)) : 0u);
+    const uint32_t rcw = lane < P.W ? lanerev32(vv) : 0u;
+    const int64_t bt = i / batch, off = i - bt * batch;
+    const int64_t nb = min(batch, nwin - bt * batch);
+    const int64_t colf = 2 * bt * batch + off, colr = colf + nb;
+    sparse_fragment<OUT, M>(P, table, warea, fw, reinterpret_cast<unsigned char *>(dest) + rowbytes * colf,
+                            norms + colf * M, scales ? scales + colf : nullptr);
+    sparse_fragment<OUT, M>(P, table, warea, rcw, reinterpret_cast<unsigned char *>(dest) + rowbytes * colr,
+                            norms + colr * M, scales ? scales + colr : nullptr);
+  }
+}
+
 __global__ void k_f32_to_e4m3(uint8_t *dst, const float *src, int64_t count) {
   int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
   int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
@@ -701,9 +1066,85 @@ static int plan_launch(EncParams &P, KernelFn kern, int64_t nwork, int *grid, in
   return R2M_OK;
 }
 
+// The sparse path serves normalize = 0 with m in {1, 2, 4, 8}, at most 255
+// distinct c-mers per fragment, whole 16-byte output chunks per c-mer run
+// and k <= 496 (the words of a fragment fit one warp's registers).  The
+// environment variable R2M_ENCODER=dense (or sparse) forces a path.
+static bool sparse_ok(const EncParams &P, int outb) {
+  const char *force = getenv("R2M_ENCODER");
+  if (force && strcmp(force, "dense") == 0) return false;
+  if (P.normalize != 0) return false;
+  if (P.m != 1 && P.m != 2 && P.m != 4 && P.m != 8) return false;
+  const int CB = P.m * outb;
+  if (CB > 16) return false;
+  const long long ncm = 1LL << (2 * P.c);
+  if (ncm * CB < 16) return false;
+  if (P.sp_nslot > 255 || P.W > 31) return false;
+  const SparseLayout L = sparse_layout(P.c, P.m, P.sp_nslot, outb);
+  return sparse_table_bytes(P) + (size_t)L.warp * 2 <= 200 * 1024;
+}
+
+template <typename KernelFn>
+static int sparse_grid(KernelFn kern, const EncParams &P, int outb, int64_t nwork, int *grid, int *block,
+                       size_t *smem) {
+  const SparseLayout L = sparse_layout(P.c, P.m, P.sp_nslot, outb);
+  int wpb = 8;
+  while (wpb > 1 && sparse_table_bytes(P) + (size_t)L.warp * wpb > 200 * 1024) wpb >>= 1;
+  *block = 32 * wpb;
+  *smem = sparse_table_bytes(P) + (size_t)L.warp * wpb;
+  R2M_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  int per_sm = 0;
+  R2M_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, *block, *smem));
+  if (per_sm < 1) per_sm = 1;
+  const int64_t want = (nwork + wpb - 1) / wpb, cap = (int64_t)sm_count() * per_sm;
+  *grid = (int)(want < cap ? want : cap);
+  if (*grid < 1) *grid = 1;
+  return R2M_OK;
+}
+
+template <int OUT, int M>
+static int launch_sparse_frags(const EncParams &P, void *dest, float *norms, float *scales, const uint32_t *dnas,
+                               int64_t n, cudaStream_t st) {
+  if constexpr (M * OutT<OUT>::bytes > 16) {
+    return fail(R2M_EINVAL, "sparse encoder: output run too wide");
+  } else {
+    int grid, block;
+    size_t smem;
+    int rc = sparse_grid(k_encode_sparse<OUT, M>, P, OutT<OUT>::bytes, n, &grid, &block, &smem);
+    if (rc) return rc;
+    k_encode_sparse<OUT, M><<<grid, block, smem, st>>>(P, dnas, n, dest, norms, scales);
+    R2M_CUDA(cudaGetLastError());
+    return R2M_OK;
+  }
+}
+
+template <int OUT, int M>
+static int launch_sparse_ref(const EncParams &P, void *dest, float *norms, float *scales, const uint32_t *genome,
+                             const int64_t *pos, int64_t nwin, int64_t batch, cudaStream_t st) {
+  if constexpr (M * OutT<OUT>::bytes > 16) {
+    return fail(R2M_EINVAL, "sparse encoder: output run too wide");
+  } else {
+    int grid, block;
+    size_t smem;
+    int rc = sparse_grid(k_encode_sparse_ref<OUT, M>, P, OutT<OUT>::bytes, nwin, &grid, &block, &smem);
+    if (rc) return rc;
+    k_encode_sparse_ref<OUT, M><<<grid, block, smem, st>>>(P, genome, pos, nwin, batch, dest, norms, scales);
+    R2M_CUDA(cudaGetLastError());
+    return R2M_OK;
+  }
+}
+
 template <int OUT>
 static int launch_frags(EncParams P, void *dest, float *norms, float *scales, const uint32_t *dnas,
                         int64_t n, cudaStream_t st) {
+  if (sparse_ok(P, OutT<OUT>::bytes)) {
+    switch (P.m) {
+      case 1: return launch_sparse_frags<OUT, 1>(P, dest, norms, scales, dnas, n, st);
+      case 2: return launch_sparse_frags<OUT, 2>(P, dest, norms, scales, dnas, n, st);
+      case 4: return launch_sparse_frags<OUT, 4>(P, dest, norms, scales, dnas, n, st);
+      default: return launch_sparse_frags<OUT, 8>(P, dest, norms, scales, dnas, n, st);
+    }
+  }
   int grid, block;
   size_t smem;
   float2 *gt = nullptr;
@@ -719,6 +1160,14 @@ static int launch_frags(EncParams P, void *dest, float *norms, float *scales, co
 template <int OUT>
 static int launch_ref(EncParams P, void *dest, float *norms, float *scales, const uint32_t *genome,
                       const int64_t *pos, int64_t nwin, int64_t batch, cudaStream_t st) {
+  if (sparse_ok(P, OutT<OUT>::bytes)) {
+    switch (P.m) {
+      case 1: return launch_sparse_ref<OUT, 1>(P, dest, norms, scales, genome, pos, nwin, batch, st);
+      case 2: return launch_sparse_ref<OUT, 2>(P, dest, norms, scales, genome, pos, nwin, batch, st);
+      case 4: return launch_sparse_ref<OUT, 4>(P, dest, norms, scales, genome, pos, nwin, batch, st);
+      default: return launch_sparse_ref<OUT, 8>(P, dest, norms, scales, genome, pos, nwin, batch, st);
+    }
+  }
   int grid, block;
   size_t smem;
   float2 *gt = nullptr;

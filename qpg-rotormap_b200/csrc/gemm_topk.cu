@@ -1215,6 +1215,17 @@ int engine_rebind(r2m_engine *eng, const uint8_t *d_B, const float *d_scaleB, in
 }
 }  // namespace r2m
 
+extern "C" int r2m_engine_info(const r2m_engine *eng, int *k, int *rdim, int *score_mode, int *rows_cap,
+                               int64_t *N) {
+  R2M_REQUIRE(eng != nullptr, "engine is null");
+  if (k) *k = eng->k;
+  if (rdim) *rdim = eng->rdim;
+  if (score_mode) *score_mode = eng->score_mode;
+  if (rows_cap) *rows_cap = eng->rows_cap;
+  if (N) *N = eng->N;
+  return R2M_OK;
+}
+
 extern "C" int64_t r2m_engine_workspace_bytes(const r2m_engine *eng) {
   if (!eng) return 0;
   return (int64_t)(eng->part_lists * eng->KT * (sizeof(float) + sizeof(int)));

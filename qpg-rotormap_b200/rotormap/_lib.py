@@ -95,6 +95,23 @@ SIGNATURES = [
     ("r2m_dreads_spans", P, [P]),
     ("r2m_dreads_header_blob", P, [P, ctypes.POINTER(SZ)]),
     ("r2m_dreads_free", None, [P]),
+    ("r2m_engine_info", I, [P, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I),
+                            ctypes.POINTER(I64)]),
+    ("r2m_server_create", I, [P, I, I, I, I, I, I64, I64, I, ctypes.POINTER(P)]),
+    ("r2m_server_submit", I, [P, P, I64, P, P, ctypes.c_double, ctypes.POINTER(I64)]),
+    ("r2m_server_submit_fasta", I, [P, ctypes.c_char_p, SZ, I, ctypes.c_double, ctypes.POINTER(I64),
+                                    ctypes.POINTER(I64)]),
+    ("r2m_server_cancel", I, [P, I64]),
+    ("r2m_server_wait", I, [P, I64, ctypes.c_double, ctypes.POINTER(I)]),
+    ("r2m_server_request", I, [P, I64, ctypes.POINTER(I), ctypes.POINTER(I64), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("r2m_server_request_error", ctypes.c_char_p, [P, I64]),
+    ("r2m_server_copy_result", I, [P, I64, P, P]),
+    ("r2m_server_reads", P, [P, I64]),
+    ("r2m_server_release", I, [P, I64]),
+    ("r2m_server_get_stats", I, [P, P]),
+    ("r2m_server_request_bytes", I64, [P, I64]),
+    ("r2m_server_destroy", I, [P, I]),
     ("r2m_jlbin_open", I, [ctypes.c_char_p, ctypes.POINTER(P)]),
     ("r2m_jlbin_parse", I, [P, SZ, ctypes.POINTER(P)]),
     ("r2m_jlbin_version", I, [P]),

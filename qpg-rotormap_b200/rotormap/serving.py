@@ -1,16 +1,22 @@
 """Serving form: a continuous-batching request loop over the resident index.
 
-Requests (packed read words of any count) arrive at any time via submit().
-The loop keeps the index and every admitted request's state resident on the
-device (its words, e4m3 rows and result lists), admits requests in arrival
-order while their state fits the HBM budget, and forms each GPU batch from
+The loop itself is native (r2m_server_*, csrc/server.cpp): requests
+(packed read words of any count, or FASTA bytes) arrive at any time via
+submit(); the library's loop thread keeps the index and every admitted
+request's state resident on the device (its words and result lists), admits
+requests in arrival order while their state fits both the byte budget and
+the device memory free at that moment, and forms each GPU batch from
 segments of all admitted requests -- a request that arrives while others are
 running joins the next batch instead of waiting for them to finish.
-Request uploads and result downloads run on a copy stream and overlap the
-fused search on the compute stream.  Every read's result is independent of
-the batch it lands in (the encoder and the fused top-k are deterministic
-per row and the top-k order is total), so a request maps to the same result
-alone and in the mix.
+Uploads and downloads run on a copy stream and overlap the fused search on
+the compute stream.  Every read's result is independent of the batch it
+lands in (the encoder and the fused top-k are deterministic per row and the
+top-k order is total), so a request maps to the same result alone and in
+the mix.  Requests can be cancelled, queued or in flight.
+
+This module is the Python client: MappingServer marshals buffers (page-
+locked, so the loop copies them asynchronously) and maps the loop's states
+to results and exceptions.
 
 The plain batch path (`plain_map`) is the reference contract for
 comparison: one request at a time, fixed batches, synchronous per batch
@@ -18,228 +24,183 @@ comparison: one request at a time, fixed batches, synchronous per batch
 """
 from __future__ import annotations
 
-import collections
-import threading
+import ctypes
 import time
-from dataclasses import dataclass, field
 
 import numpy as np
 import torch
 
+from ._lib import R2MError, R2M_ENOMEM, check, lib
 from .encoder import RopeEncoder, encode_frag_real_batch
 
+QUEUED, ACTIVE, DONE, CANCELLED, FAILED = 0, 1, 2, 3, 4
 
-@dataclass
+
+class CancelledError(RuntimeError):
+    pass
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("batches", "rows", "max_rows", "requests_done",
+                                              "requests_cancelled", "requests_failed", "in_use_bytes",
+                                              "peak_in_use_bytes", "queued", "active")]
+
+
 class Request:
-    rid: int
-    n: int
-    words_h: np.ndarray
-    t_arrival: float
-    heads: list | None = None
-    t_admit: float = 0.0
-    t_done: float = 0.0
-    vals: np.ndarray | None = None
-    locs: np.ndarray | None = None
-    error: str | None = None
-    # device state
-    words_d: torch.Tensor | None = None
-    vals_d: torch.Tensor | None = None
-    locs_d: torch.Tensor | None = None
-    uploaded: torch.cuda.Event | None = None
-    scheduled: int = 0
-    completed: int = 0
-    nbytes: int = 0
-    done: threading.Event = field(default_factory=threading.Event)
+    """A submitted request: result() waits for it (CLOCK_MONOTONIC times,
+    the clock of time.perf_counter on Linux)."""
+
+    def __init__(self, srv, rid: int, n: int, k: int, vals=None, locs=None, words=None, fasta: bool = False):
+        self._srv, self.rid, self.n, self.k = srv, rid, n, k
+        self._vals, self._locs, self._words = vals, locs, words  # pinned buffers the loop writes / reads
+        self.fasta = fasta
+        self._out = None
+
+    def _times(self):
+        st, n = ctypes.c_int(), ctypes.c_int64()
+        ta, tad, td = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().r2m_server_request(self._srv._h, self.rid, ctypes.byref(st), ctypes.byref(n),
+                                       ctypes.byref(ta), ctypes.byref(tad), ctypes.byref(td)))
+        return st.value, ta.value, tad.value, td.value
+
+    @property
+    def state(self) -> int:
+        return self._times()[0]
+
+    @property
+    def t_arrival(self) -> float:
+        return self._times()[1]
+
+    @property
+    def t_admit(self) -> float:
+        return self._times()[2]
+
+    @property
+    def t_done(self) -> float:
+        return self._times()[3]
 
     @property
     def latency(self) -> float:
-        return self.t_done - self.t_arrival
+        _, ta, _, td = self._times()
+        return td - ta
+
+    def cancel(self) -> None:
+        check(lib().r2m_server_cancel(self._srv._h, self.rid))
 
     def result(self, timeout: float | None = None):
-        if not self.done.wait(timeout):
-            raise TimeoutError(f"request {self.rid} not done")
-        if self.error:
-            raise RuntimeError(self.error)
-        return self.vals, self.locs
+        if self._out is not None:
+            return self._out
+        st = ctypes.c_int()
+        rc = lib().r2m_server_wait(self._srv._h, self.rid, -1.0 if timeout is None else float(timeout),
+                                   ctypes.byref(st))
+        if rc != 0:
+            if st.value in (QUEUED, ACTIVE):
+                raise TimeoutError(f"request {self.rid} not done")
+            check(rc)
+        if st.value == CANCELLED:
+            raise CancelledError(f"request {self.rid} was cancelled")
+        if st.value == FAILED:
+            msg = lib().r2m_server_request_error(self._srv._h, self.rid)
+            raise RuntimeError(msg.decode() if msg else "request failed")
+        if self.fasta:
+            v = np.empty((self.n, self.k), np.float32)
+            l = np.empty((self.n, self.k), np.int32)
+            check(lib().r2m_server_copy_result(self._srv._h, self.rid, v.ctypes.data, l.ctypes.data))
+            self._out = (v, l)
+        else:
+            self._out = (self._vals.numpy(), self._locs.numpy())
+        return self._out
+
+    def headers(self) -> list:
+        """The parsed reads' headers of a FASTA request."""
+        h = lib().r2m_server_reads(self._srv._h, self.rid)
+        if not h:
+            return []
+        tot = ctypes.c_size_t()
+        p = lib().r2m_reads_header_blob(h, ctypes.byref(tot))
+        return ctypes.string_at(p, tot.value).decode("latin-1").split("\n")[:self.n]
 
 
 class MappingServer:
-    """Continuous-batching mapper over a fused TopKEngine."""
+    """Continuous-batching mapper over a fused TopKEngine (native loop)."""
 
     def __init__(self, eng, re: RopeEncoder, hbm_budget: int | None = None, normalize: int = 0,
-                 max_queued_batches: int = 2):
+                 max_queued_batches: int = 2, hbm_reserve: int = 1 << 30):
         self.eng, self.re, self.normalize = eng, re, normalize
         self.dev = eng.device
         self.k = eng.k
         self.cap = eng.rows_cap
-        self.scaled = eng.score == "scaled"
-        free, _ = torch.cuda.mem_get_info(self.dev)
-        self.budget = hbm_budget if hbm_budget is not None else int(free * 0.5)
-        self.in_use = 0
-        self.comp = torch.cuda.Stream(self.dev)
-        self.copy = torch.cuda.Stream(self.dev)
-        self.max_queued = max_queued_batches
-        # one batch slot: stream order on `comp` serialises its reuse
-        self.norms = torch.empty((self.cap, re.m), dtype=torch.float32, device=self.dev)
-        self.vals = torch.empty((self.cap, self.k), dtype=torch.float32, device=self.dev)
-        self.locs = torch.empty((self.cap, self.k), dtype=torch.int32, device=self.dev)
-        self._lock = threading.Condition()
-        self._waiting: collections.deque = collections.deque()
-        self._active: list = []
-        self._inflight: collections.deque = collections.deque()  # (event, [(req, lo, n)])
-        self._downloads: collections.deque = collections.deque()  # (event, req)
-        self._next_id = 0
-        self._stop = False
-        self.batches = 0
-        self.batch_rows = []
-        self._thread = threading.Thread(target=self._loop, name="rotormap-serving", daemon=True)
-        self._thread.start()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.dev):
+            check(lib().r2m_server_create(eng._h, re.k, re.s, re.m, re.c, normalize,
+                                          int(hbm_budget) if hbm_budget else 0, int(hbm_reserve),
+                                          int(max_queued_batches), ctypes.byref(h)))
+        self._h = h
+        self.budget = int(hbm_budget) if hbm_budget else 0
 
     # ------------------------------------------------------------ client API
 
     def request_bytes(self, n: int) -> int:
-        return n * (self.re.words * 4 + self.k * 8)
+        return int(lib().r2m_server_request_bytes(self._h, n))
 
     def submit(self, words: np.ndarray, heads=None, t_arrival: float | None = None) -> Request:
         words = np.ascontiguousarray(words, dtype=np.uint32)
         if words.ndim != 2 or words.shape[1] != self.re.words:
             raise ValueError(f"words must be (n, {self.re.words}) uint32")
         n = words.shape[0]
-        nbytes = self.request_bytes(n)
-        if nbytes > self.budget:
-            raise MemoryError(f"request of {n} reads needs {nbytes} B > the HBM budget {self.budget} B")
-        with self._lock:
-            r = Request(self._next_id, n, words, t_arrival if t_arrival is not None else time.perf_counter(),
-                        heads, nbytes=nbytes)
-            self._next_id += 1
-            if n == 0:
-                r.vals = np.zeros((0, self.k), np.float32)
-                r.locs = np.zeros((0, self.k), np.int32)
-                r.t_done = time.perf_counter()
-                r.done.set()
-                return r
-            self._waiting.append(r)
-            self._lock.notify_all()
+        hw = torch.from_numpy(words.reshape(-1).view(np.int32)).pin_memory()
+        hv = torch.empty((n, self.k), dtype=torch.float32, pin_memory=True)
+        hl = torch.empty((n, self.k), dtype=torch.int32, pin_memory=True)
+        rid = ctypes.c_int64()
+        rc = lib().r2m_server_submit(self._h, hw.data_ptr() if n else None, n, hv.data_ptr() if n else None,
+                                     hl.data_ptr() if n else None, float(t_arrival or 0.0), ctypes.byref(rid))
+        if rc == R2M_ENOMEM:
+            raise MemoryError(lib().r2m_last_error().decode())
+        check(rc)
+        r = Request(self, rid.value, n, self.k, hv, hl, hw)
+        r.heads = heads
         return r
 
+    def submit_fasta(self, data: bytes, t_arrival: float | None = None, nthreads: int = 4) -> Request:
+        rid, n = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().r2m_server_submit_fasta(self._h, data, len(data), nthreads, float(t_arrival or 0.0),
+                                            ctypes.byref(rid), ctypes.byref(n)))
+        return Request(self, rid.value, n.value, self.k, fasta=True)
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib().r2m_server_get_stats(self._h, ctypes.byref(st)))
+        return st
+
+    @property
+    def batches(self) -> int:
+        return self.stats().batches
+
+    @property
+    def in_use(self) -> int:
+        return self.stats().in_use_bytes
+
     def close(self, wait: bool = True):
-        with self._lock:
-            self._stop = True
-            self._lock.notify_all()
-        if wait:
-            self._thread.join()
+        if self._h:
+            h, self._h = self._h, None
+            check(lib().r2m_server_destroy(h, 0 if wait else 1))
 
     def drain(self, timeout: float = 600.0):
-        """Block until every submitted request has completed."""
+        """Block until every submitted request has finished."""
         t0 = time.perf_counter()
-        with self._lock:
-            while self._waiting or self._active or self._inflight or self._downloads:
-                if time.perf_counter() - t0 > timeout:
-                    raise TimeoutError("serving loop did not drain")
-                self._lock.wait(0.01)
-
-    # ------------------------------------------------------------ the loop
-
-    def _admit(self):
-        while self._waiting and self.in_use + self._waiting[0].nbytes <= self.budget:
-            r = self._waiting.popleft()
-            r.t_admit = time.perf_counter()
-            self.in_use += r.nbytes
-            with torch.cuda.stream(self.copy):
-                hw = torch.from_numpy(r.words_h.reshape(-1).view(np.int32)).pin_memory()
-                r.words_d = hw.to(self.dev, non_blocking=True)
-                r.vals_d = torch.empty((r.n, self.k), dtype=torch.float32, device=self.dev)
-                r.locs_d = torch.empty((r.n, self.k), dtype=torch.int32, device=self.dev)
-                r.uploaded = torch.cuda.Event()
-                r.uploaded.record(self.copy)
-            r._pinned = hw  # keep the staging alive until the copy ran
-            self._active.append(r)
-
-    def _launch_batch(self):
-        segs, off = [], 0
-        for r in self._active:
-            if off >= self.cap:
-                break
-            left = r.n - r.scheduled
-            if left <= 0:
-                continue
-            take = min(left, self.cap - off)
-            segs.append((r, r.scheduled, take, off))
-            r.scheduled += take
-            off += take
-        if not segs:
-            return False
-        nb = off
-        eng, W = self.eng, self.re.words
-        with torch.cuda.stream(self.comp):
-            for r, lo, n, o in segs:
-                self.comp.wait_event(r.uploaded)
-                sa = eng.scaleA[o:o + n] if self.scaled else None
-                encode_frag_real_batch(eng.a8[o:o + n], self.norms[o:o + n], self.re,
-                                       r.words_d[lo * W:(lo + n) * W], self.normalize, sa, self.comp)
-            eng.search(eng.a8[:nb], nb, eng.scaleA[:nb] if self.scaled else None, self.vals[:nb],
-                       self.locs[:nb], self.comp)
-            for r, lo, n, o in segs:
-                r.vals_d[lo:lo + n].copy_(self.vals[o:o + n], non_blocking=True)
-                r.locs_d[lo:lo + n].copy_(self.locs[o:o + n], non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(self.comp)
-        self._inflight.append((ev, [(r, lo, n) for r, lo, n, _ in segs]))
-        self.batches += 1
-        self.batch_rows.append(nb)
-        return True
-
-    def _retire(self):
-        progressed = False
-        while self._inflight and self._inflight[0][0].query():
-            _, segs = self._inflight.popleft()
-            progressed = True
-            for r, lo, n in segs:
-                r.completed += n
-                if r.completed == r.n:
-                    with torch.cuda.stream(self.copy):
-                        r.vals = torch.empty((r.n, self.k), dtype=torch.float32, pin_memory=True)
-                        r.locs = torch.empty((r.n, self.k), dtype=torch.int32, pin_memory=True)
-                        r.vals.copy_(r.vals_d, non_blocking=True)
-                        r.locs.copy_(r.locs_d, non_blocking=True)
-                        ev = torch.cuda.Event()
-                        ev.record(self.copy)
-                    self._downloads.append((ev, r))
-            self._active = [r for r in self._active if r.completed < r.n]
-        while self._downloads and self._downloads[0][0].query():
-            _, r = self._downloads.popleft()
-            r.t_done = time.perf_counter()
-            r.vals, r.locs = r.vals.numpy(), r.locs.numpy()
-            self.in_use -= r.nbytes
-            r.words_d = r.vals_d = r.locs_d = None
-            r._pinned = None
-            r.done.set()
-            progressed = True
-        return progressed
-
-    def _loop(self):
-        torch.cuda.set_device(self.dev)
         while True:
-            with self._lock:
-                if self._stop and not (self._waiting or self._active or self._inflight or self._downloads):
-                    return
-                try:
-                    progressed = self._retire()
-                    self._admit()
-                    launched = False
-                    if len(self._inflight) < self.max_queued:
-                        launched = self._launch_batch()
-                except Exception as e:  # fail every pending request, keep the loop alive
-                    for r in list(self._waiting) + self._active:
-                        r.error = f"{type(e).__name__}: {e}"
-                        r.done.set()
-                    self._waiting.clear()
-                    self._active.clear()
-                    progressed, launched = True, False
-                if not (progressed or launched):
-                    self._lock.wait(0.0005)
-                else:
-                    self._lock.notify_all()
+            st = self.stats()
+            if st.queued == 0 and st.active == 0:
+                return
+            if time.perf_counter() - t0 > timeout:
+                raise TimeoutError("serving loop did not drain")
+            time.sleep(0.001)
+
+    def __del__(self):
+        try:
+            self.close(wait=False)
+        except Exception:
+            pass
 
 
 def plain_map(eng, re: RopeEncoder, requests, batch: int = 8192, normalize: int = 0, clock=None):

@@ -205,3 +205,68 @@ def test_reference_experiment_curves_through_the_gpu_encoder():
     assert abs(sr - sweep["shift_anchor"]["ip_re"]) < 1e-4 and abs(sa - sweep["shift_anchor"]["ip_abs"]) < 1e-4
     for j in range(2, len(muts)):
         assert np.allclose(ip(g[0], g[j]), ip(o[0], o[j]), rtol=0, atol=1e-5)
+
+
+SPARSE_CONFIGS = [(150, 8, 4, 4), (100, 8, 4, 4), (250, 8, 4, 4), (37, 5, 1, 3), (20, 8, 2, 2), (60, 6, 8, 3)]
+
+
+@pytest.mark.parametrize("k,s,m,c", SPARSE_CONFIGS)
+def test_sparse_and_dense_encoders_agree(k, s, m, c, monkeypatch):
+    """The slot-based encoder (normalize 0, the default at read length) and
+    the dense-histogram encoder form every bin as the same sum in the same
+    order: fp32 rows agree to the rounding of the norm's summation order,
+    and each path's fp16 / e4m3 outputs are the conversions of its own fp32
+    values."""
+    rng = np.random.default_rng(k + 7 * m)
+    words = random_words(rng, 300, k)
+    re = rm.RopeEncoder(k=k, s=s, m=m, c=c)
+    outs = {}
+    for path in ("sparse", "dense"):
+        monkeypatch.setenv("R2M_ENCODER", path)
+        f32, n32 = _gpu_encode(words, re)
+        e8, _ = _gpu_encode(words, re, dtype=torch.uint8)
+        s8, _, sc = _gpu_encode(words, re, dtype=torch.uint8, scaled=True)
+        assert np.array_equal(e8, orc.quantize_parity(f32))
+        q, scale = orc.quantize_scaled(f32)
+        assert np.array_equal(s8, q) and np.array_equal(sc, scale)
+        outs[path] = (f32, n32)
+    (a, na), (b, nb) = outs["sparse"], outs["dense"]
+    np.testing.assert_allclose(a, b, rtol=2e-6, atol=1e-8)
+    np.testing.assert_allclose(na, nb, rtol=2e-6)
+    o32, _ = orc.rope_f32(words, k, s, m, c)
+    np.testing.assert_allclose(a, o32, rtol=RTOL_F32, atol=ATOL_F32)
+
+
+def test_sparse_index_windows_equal_dense(monkeypatch):
+    """Index columns (forward and reverse complement from the packed
+    genome, register-formed on the sparse path) from both encoders."""
+    from rotormap import synth
+    from rotormap._lib import OUT_E4M3_SCALED, check, lib, ptr
+    recs = synth.random_genome([5000, 777, 3000], seed=4, n_frac=0.02, run_min=10, run_max=40)
+    heads = [">a", ">b", ">c"]
+    fa = synth.genome_fasta(heads, recs)
+    for k in (150, 100, 37):
+        pack = rm.pack_reference(fa)
+        pos, _, _ = rm.window_positions(pack, k, 7)
+        nwin = pos.size
+        g = torch.from_numpy(pack.words.view(np.int32)).cuda()
+        p = torch.from_numpy(pos).cuda()
+        res = {}
+        for path in ("sparse", "dense"):
+            monkeypatch.setenv("R2M_ENCODER", path)
+            out = torch.empty((2 * nwin, 2048), dtype=torch.uint8, device="cuda")
+            nrm = torch.empty((2 * nwin, 4), dtype=torch.float32, device="cuda")
+            sc = torch.empty((2 * nwin,), dtype=torch.float32, device="cuda")
+            check(lib().r2m_encode_ref_windows(ptr(out), OUT_E4M3_SCALED, ptr(nrm), ptr(sc), ptr(g), ptr(p), nwin,
+                                               100, k, 8, 4, 4, 0, torch.cuda.current_stream().cuda_stream))
+            torch.cuda.synchronize()
+            res[path] = (out.cpu().numpy(), nrm.cpu().numpy(), sc.cpu().numpy())
+        (a, na, sa), (b, nb, sb) = res["sparse"], res["dense"]
+        np.testing.assert_allclose(na, nb, rtol=2e-6)
+        np.testing.assert_allclose(sa, sb, rtol=2e-6)
+        # a norm rounded differently can move a value across an e4m3 rounding
+        # boundary: at most one step, in a tiny share of the bytes
+        diff = a != b
+        assert diff.mean() < 1e-4
+        t = orc.e4m3_table()
+        assert np.all(np.abs(t[a[diff]] - t[b[diff]]) <= np.abs(t[b[diff]]) * 0.13 + 1e-9)
