@@ -111,11 +111,13 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        pw = [float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
                           and "Not" not in r[5 + i]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows),
+                "power_w": statistics.median(pw) if pw else None}
 
 
 def peaks():
@@ -555,16 +557,22 @@ def gemm_bar_leg(dev, seconds: float = 2.0):
     e1.synchronize()
     burst_ms = e0.elapsed_time(e1) / 20
     reps = max(20, int(seconds * 1e3 / max(burst_ms, 1e-3)))
+    clk = Clocks(dev.index if dev.index is not None else 0)
+    clk.start()
     e0.record()
     for _ in range(reps):
         run()
     e1.record()
     e1.synchronize()
+    c = clk.stop()
     sus_ms = e0.elapsed_time(e1) / reps
     flop = 2.0 * M * K * N
+    sus = flop / sus_ms / 1e9
     return {"library": "cuBLASLt fp8 via torch._scaled_mm", "shape": {"M": M, "K": K, "N": N},
             "out": "fp16", "burst_ms": burst_ms, "burst_tflops": flop / burst_ms / 1e9,
-            "sustained_ms": sus_ms, "sustained_tflops": flop / sus_ms / 1e9, "sustained_calls": reps}
+            "sustained_ms": sus_ms, "sustained_tflops": sus, "sustained_calls": reps,
+            "sustained_clocks": c,
+            "tflops_per_w": sus / c["power_w"] if c.get("power_w") else None}
 
 
 def map_leg(dev, n_reads: int = 400_000, ncols: int = 1_048_576, seed: int = 91):
@@ -856,6 +864,11 @@ def main():
         flops = 2.0 * nq * N * re.rdim
         achieved = flops / (g_avg * 1e-3) / 1e12
         enc_bytes = nq * (re.words * 4 + re.rdim + 4 + 4 * M)
+        # tensor-pipe estimate from the clock: the dense fp8 rate of an SM's
+        # tensor pipe, 16,384 FLOP per clock (x 148 SMs x ~1.86 GHz = the
+        # nominal 4.5 PFLOP/s), times the SMs and the sampled median clock
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        pipe_peak = 16384.0 * sms * (clk["sm_mhz"] or 0) * 1e6 / 1e12 if clk.get("sm_mhz") else None
         line = {
             "metric": METRIC, "value": nq * world / (ms * 1e-3), "unit": "reads/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
@@ -876,7 +889,12 @@ def main():
                          "kernel": ("k_gemm_topk2 (CTA-pair tcgen05 fp8 GEMM + fused top-20)" if nq > 128 else
                                     "k_gemm_topk (single-CTA tcgen05 fp8 GEMM + fused top-20)"),
                          "peak_basis": f"dense fp8 = 2 x {basis} sustained bf16 "
-                                       f"({pk['bf16_tflops_sustained']} TFLOP/s)"},
+                                       f"({pk['bf16_tflops_sustained']} TFLOP/s)",
+                         "tensor_pipe": {"est_active_frac": achieved / pipe_peak if pipe_peak else None,
+                                         "basis": "achieved / (16384 dense fp8 FLOP per SM per clock x SMs x "
+                                                  "median sampled SM clock)",
+                                         "sm_mhz": clk.get("sm_mhz")},
+                         "tflops_per_w": achieved / clk["power_w"] if clk.get("power_w") else None},
             "encoder": {"ms": sum(enc_ms) / len(enc_ms),
                         "achieved_gbs": enc_bytes / (sum(enc_ms) / len(enc_ms) * 1e-3) / 1e9,
                         "peak_gbs": pk["hbm_gbs"]},

@@ -447,28 +447,52 @@ def topk_flow(source, eng: TopKEngine, re: RopeEncoder, normalize: int = 0, stre
         yield TopKBatch(vals.numpy(), locs.numpy(), nrm.numpy(), heads, first0 + 1)
 
 
+HOST_READER_MAX_BYTES = 8 << 30  # inputs the host reader takes whole
+
+
+def pick_reader(file, reader: str = "auto") -> str:
+    """reader = "auto": the native host reader when the host has >= 8 threads
+    and the input is at most 8 GiB (it parses the whole input at once; its
+    words then cross to the device at 40 bytes per 150 bp read, against ~190
+    bytes of FASTA for the GPU reader -- measured faster end to end, 5.9 vs
+    3.4 GB/s from host bytes), else the GPU reader, which streams any input
+    size through bounded memory."""
+    if reader != "auto":
+        return reader
+    import os
+    if isinstance(file, (bytes, bytearray, memoryview)):
+        size = len(file)
+    else:
+        try:
+            size = os.path.getsize(file)
+        except OSError:
+            return "device"
+    return "host" if (os.cpu_count() or 1) >= 8 and size <= HOST_READER_MAX_BYTES else "device"
+
+
 def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int | None = None,
                      batch_size: int = 8192, rows_cap: int | None = None, normalize: int = 0,
                      score: str = "f16", scaleB: torch.Tensor | None = None, parts: int | None = None,
                      segs: int | None = None, engine: TopKEngine | None = None, stream=None,
-                     reader: str = "device", chunk_bytes: int = 1 << 30):
+                     reader: str = "auto", chunk_bytes: int = 1 << 30):
     """rope_topk_stream (engine_fp8.jl:576-594): FASTA -> encode -> fp8 GEMM +
     top-k against the resident B -> TopKBatch per batch (file order).
 
-    reader = "device" parses the FASTA on the GPU (the words stay in HBM),
+    reader = "auto" picks one of the two (pick_reader); "device" parses the FASTA on the GPU (the words stay in HBM),
     `chunk_bytes` of the file at a time (cut at record starts), so inputs of
     any size stream through bounded memory; "host" uses the native host
     reader with `parts` threads on the whole input.  Both give the same
     reads."""
     if B.shape[1] != re.rdim:
         raise ValueError(f"B is {tuple(B.shape)}; the encoder's real embedding dim is {re.rdim}")
+    reader = pick_reader(file, reader)
     if reader == "device":
         source = _chunked_batches(fasta_chunks_device(file, k=re.k, chunk_bytes=chunk_bytes, device=B.device,
                                                       stream=stream), batch_size)
     elif reader == "host":
         source = _batches(fasta_reads(file, k=re.k, parts=parts), batch_size)
     else:
-        raise ValueError('reader must be "device" or "host"')
+        raise ValueError('reader must be "auto", "device" or "host"')
     eng = engine or TopKEngine(B, k=k, rows_cap=rows_cap or batch_size, score=score, scaleB=scaleB)
     yield from topk_flow(source, eng, re, normalize, stream)
 
@@ -489,7 +513,7 @@ def resident_fits(host_bytes: int, rows_cap: int, rdim: int, k: int = 20, device
 def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size: int = 8192,
                              rows_cap: int | None = None, normalize: int = 0, score: str = "f16",
                              scaleB=None, resident: bool | None = None, chunk_cols: int = 1 << 20,
-                             depth: int = 3, pin: bool = True, reader: str = "device", parts: int | None = None,
+                             depth: int = 3, pin: bool = True, reader: str = "auto", parts: int | None = None,
                              stream=None, resident_chunks="auto"):
     """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index
     Bh (N, rdim) uint8.  resident = None applies resident_fits: an index that
@@ -520,13 +544,14 @@ def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size:
     eng = CompactEngine(Bh, k=k, rows_cap=cap, score=score, scaleB=sb, chunk_cols=chunk_cols, depth=depth,
                         pin=pin, resident_chunks=resident_chunks)
     try:
+        reader = pick_reader(file, reader)
         if reader == "device":
             source = _chunked_batches(fasta_chunks_device(file, k=re.k, device=eng.device, stream=stream),
                                       batch_size)
         elif reader == "host":
             source = _batches(fasta_reads(file, k=re.k, parts=parts), batch_size)
         else:
-            raise ValueError('reader must be "device" or "host"')
+            raise ValueError('reader must be "auto", "device" or "host"')
         yield from topk_flow(source, eng, re, normalize, stream)
     finally:
         eng.close()

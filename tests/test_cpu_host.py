@@ -465,3 +465,18 @@ def test_package_modules_bind_every_name_they_load():
         missing = sorted(u for u in used if u not in bound and not hasattr(builtins, u)
                          and u not in ("__file__", "__name__"))
         assert not missing, f"{path.name}: {missing}"
+
+
+def test_pick_reader_follows_the_faster_path(tmp_path, monkeypatch):
+    """reader="auto": the host reader on a host with >= 8 threads for inputs
+    up to 8 GiB, else the GPU reader (which streams any size)."""
+    import os
+    from rotormap.engine import pick_reader
+    p = tmp_path / "r.fa"
+    p.write_bytes(b">r\nACGT\n")
+    assert pick_reader(str(p), "device") == "device" and pick_reader(str(p), "host") == "host"
+    monkeypatch.setattr(os, "cpu_count", lambda: 16)
+    assert pick_reader(str(p)) == "host" and pick_reader(b">r\nAC\n") == "host"
+    assert pick_reader(str(tmp_path / "missing.fa")) == "device"
+    monkeypatch.setattr(os, "cpu_count", lambda: 2)
+    assert pick_reader(str(p)) == "device"
