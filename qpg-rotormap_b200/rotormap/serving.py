@@ -97,6 +97,7 @@ class Request:
             if st.value in (QUEUED, ACTIVE):
                 raise TimeoutError(f"request {self.rid} not done")
             check(rc)
+        self._srv._live.pop(self.rid, None)  # finished: the loop no longer touches its buffers
         if st.value == CANCELLED:
             raise CancelledError(f"request {self.rid} was cancelled")
         if st.value == FAILED:
@@ -137,6 +138,7 @@ class MappingServer:
                                           int(max_queued_batches), ctypes.byref(h)))
         self._h = h
         self.budget = int(hbm_budget) if hbm_budget else 0
+        self._live: dict = {}
 
     # ------------------------------------------------------------ client API
 
@@ -159,6 +161,7 @@ class MappingServer:
         check(rc)
         r = Request(self, rid.value, n, self.k, hv, hl, hw)
         r.heads = heads
+        self._live[r.rid] = r  # the loop reads and writes its buffers until it finishes
         return r
 
     def submit_fasta(self, data: bytes, t_arrival: float | None = None, nthreads: int = 4) -> Request:
@@ -183,7 +186,10 @@ class MappingServer:
     def close(self, wait: bool = True):
         if self._h:
             h, self._h = self._h, None
-            check(lib().r2m_server_destroy(h, 0 if wait else 1))
+            try:
+                check(lib().r2m_server_destroy(h, 0 if wait else 1))
+            finally:
+                self._live.clear()  # the loop has stopped: buffers are free to go
 
     def drain(self, timeout: float = 600.0):
         """Block until every submitted request has finished."""

@@ -16,7 +16,7 @@ rope_shift_mutation_sweep.csv, err = 0: the pristine fragment against its
 500-base shifted copy, same encoder) is kept verbatim as a second,
 near-deterministic anchor.
 
-Usage: python tests/golden/make_sweep_bins.py [path/to/reference/checkout]
+Usage: python tests/golden/make_sweep_bins.py path/to/reference/checkout
 """
 import csv
 import json
@@ -29,7 +29,9 @@ NBINS = 20
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_sweep_bins.py path/to/reference/checkout")
+    root = Path(sys.argv[1])
     src = root / "RotorMap" / "experiments" / "out" / "rope_mutation_sweep.csv"
     rows = list(csv.DictReader(open(src)))
     err = np.array([float(r["err"]) for r in rows])

@@ -7,6 +7,7 @@ import pytest
 import torch
 
 from oracle import oracle as orc
+from topk_check import assert_topk_rows, oracle_scores_at
 
 import rotormap as rm
 
@@ -54,6 +55,6 @@ def test_plain_path_agrees_with_fused_engine_on_realistic_data():
     eng = rm.TopKEngine(B, k=20, rows_cap=nb, score="f16")
     fv, fl = eng.search(torch.from_numpy(A8).cuda())
     fv, fl = fv.cpu().numpy(), fl.cpu().numpy()
-    np.testing.assert_allclose(v, fv, rtol=0, atol=1e-3)  # fp16 scores: one step at most
-    agree = np.mean([len(set(l[r]) & set(fl[r])) / 20 for r in range(nb)])
-    assert agree > 0.97  # remaining differences: ties and one-step boundaries
+    # fp16 scores: the two paths may differ by one fp16 step (2^-10 near 1);
+    # every location where they differ must be a tie within that step
+    assert_topk_rows(v, l, fv, fl, oracle_scores_at(A8, B8, l, 0), tol=1e-3, N=N)
