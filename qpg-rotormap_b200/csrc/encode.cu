@@ -764,6 +764,38 @@ __host__ __device__ inline SparseLayout sparse_layout(int c, int m, int nslot, i
   return L;
 }
 
+// The m complex values of one slot (or of one window's phasors) live in
+// planes: plane j holds copies 2j and 2j+1 of every slot as one 16-byte
+// entry (m = 1: one plane of 8-byte entries).  Lanes that touch consecutive
+// slots then read consecutive 16 bytes, and random slots spread over the
+// banks instead of falling on the same few (a slot-major 32-byte record
+// puts every slot on one of 4 bank groups).
+template <int M>
+__device__ __forceinline__ void ld_planes(const float2 *base, int stride, int i, float2 (&v)[M]) {
+  if constexpr (M == 1) {
+    v[0] = base[i];
+  } else {
+    const float4 *b4 = reinterpret_cast<const float4 *>(base);
+#pragma unroll
+    for (int j = 0; j < M / 2; ++j) {
+      const float4 t = b4[(size_t)j * stride + i];
+      v[2 * j] = make_float2(t.x, t.y);
+      v[2 * j + 1] = make_float2(t.z, t.w);
+    }
+  }
+}
+template <int M>
+__device__ __forceinline__ void st_planes(float2 *base, int stride, int i, const float2 (&v)[M]) {
+  if constexpr (M == 1) {
+    base[i] = v[0];
+  } else {
+    float4 *b4 = reinterpret_cast<float4 *>(base);
+#pragma unroll
+    for (int j = 0; j < M / 2; ++j)
+      b4[(size_t)j * stride + i] = make_float4(v[2 * j].x, v[2 * j].y, v[2 * j + 1].x, v[2 * j + 1].y);
+  }
+}
+
 // Encode the fragment whose W words are in `wreg` (lane t: word t, zero for
 // t >= W) with one warp into `row`, its m norms and (scaled) its row scale.
 template <int OUT, int M>
@@ -774,6 +806,7 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   using T = typename Bytes<CB>::T;
   using TM = typename Bytes<CPC>::T;
   const SparseLayout L = sparse_layout(P.c, M, P.sp_nslot, OUTB);
+  const int ns = P.sp_nslot;  // entries per accumulator plane
   uint8_t *smap = warea;
   float2 *acc = reinterpret_cast<float2 *>(warea + L.smap);
   T *conv_re = reinterpret_cast<T *>(warea + L.smap + L.acc);
@@ -809,31 +842,20 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
     nslots += __popc(newm);
     const int slot = __shfl_sync(FULL, s_l, __ffs(grp) - 1);
     float2 ph[M];
-    if (valid) {
-      if constexpr (M == 1) {
-        ph[0] = table[p];
-      } else {
-        const float4 *t4 = reinterpret_cast<const float4 *>(table + (size_t)p * M);
-#pragma unroll
-        for (int q = 0; q < M / 2; ++q) {
-          const float4 t = t4[q];
-          ph[2 * q] = make_float2(t.x, t.y);
-          ph[2 * q + 1] = make_float2(t.z, t.w);
-        }
-      }
-    }
+    if (valid) ld_planes<M>(table, P.nw, p, ph);
     const int rounds = (int)__reduce_max_sync(FULL, valid ? (unsigned)rank : 0u);
     for (int r = 0; r <= rounds; ++r) {
       if (valid && rank == r) {
-        float2 *a = acc + (size_t)slot * M;
+        float2 a[M];
         if (r == 0 && isnew) {
-          const float2 z = make_float2(0.f, 0.f);  // 0 + x, as a cleared histogram bin
 #pragma unroll
-          for (int q = 0; q < M; ++q) a[q] = add2(z, ph[q]);
+          for (int q = 0; q < M; ++q) a[q] = make_float2(0.f, 0.f);  // 0 + x, as a cleared bin
         } else {
-#pragma unroll
-          for (int q = 0; q < M; ++q) a[q] = add2(a[q], ph[q]);
+          ld_planes<M>(acc, ns, slot, a);
         }
+#pragma unroll
+        for (int q = 0; q < M; ++q) a[q] = add2(a[q], ph[q]);
+        st_planes<M>(acc, ns, slot, a);
       }
       __syncwarp();
     }
@@ -842,8 +864,10 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   if (lane == 0) {
     const int sg = smap[P.csmerG];
     if (sg != 0xFF) {
+      float2 z[M];
 #pragma unroll
-      for (int q = 0; q < M; ++q) acc[(size_t)sg * M + q] = make_float2(0.f, 0.f);
+      for (int q = 0; q < M; ++q) z[q] = make_float2(0.f, 0.f);
+      st_planes<M>(acc, ns, sg, z);
     }
   }
   __syncwarp();
@@ -852,9 +876,11 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
 #pragma unroll
   for (int q = 0; q < M; ++q) part[q] = 0.f;
   for (int sl = lane; sl < nslots; sl += 32) {
+    float2 zv[M];
+    ld_planes<M>(acc, ns, sl, zv);
 #pragma unroll
     for (int q = 0; q < M; ++q) {
-      const float2 z = acc[(size_t)sl * M + q];
+      const float2 z = zv[q];
       part[q] += __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
       mx = fmaxf(mx, fmaxf(fabsf(z.x), fabsf(z.y)));
     }
@@ -888,9 +914,11 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   // ---- convert each slot once
   for (int sl = lane; sl < nslots; sl += 32) {
     float re[M], im[M];
+    float2 xv[M];
+    ld_planes<M>(acc, ns, sl, xv);
 #pragma unroll
     for (int q = 0; q < M; ++q) {
-      const float2 x = acc[(size_t)sl * M + q];
+      const float2 x = xv[q];
       const float2 q0 = mul2(x, y2);
       float2 d = fma2(fma2(q0, nn2, x), y2, q0);
       if constexpr (OUT == R2M_OUT_E4M3_SCALED) d = mul2(d, sc2);
@@ -928,11 +956,16 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   __syncwarp();
 }
 
-// Phasor table of the sparse path: entry p * m + idm (the m copies of a
-// window side by side), the reference thread's exact fp32 values.
+// Phasor table of the sparse path, in planes (see ld_planes): copies 2j and
+// 2j+1 of window p are entry p of plane j; the reference thread's exact
+// fp32 values.
 __device__ __forceinline__ void sparse_table(const EncParams &P, float2 *t) {
   const int total = P.m * P.nw;
-  for (int i = threadIdx.x; i < total; i += blockDim.x) t[i] = ref_phasor(P, i % P.m, i / P.m);
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int idm = i / P.nw, p = i - idm * P.nw;
+    const int at = P.m == 1 ? p : (idm >> 1) * 2 * P.nw + 2 * p + (idm & 1);
+    t[at] = ref_phasor(P, idm, p);
+  }
   __syncthreads();
 }
 

@@ -40,22 +40,24 @@ class Autotuner:
     CTAs (around the built-in heuristic), the kernel (single CTAs or CTA
     pairs), the epilogue form (4 or 8 warps), the pair pacing window and the
     top-k reservoir size -- coordinate descent from the defaults, one knob at
-    a time, each kept only when it beats the best so far.
+    a time, each kept only when it beats the best so far by `min_gain`.
 
     Cost: every candidate is one warm-up and `reps` timed searches.  When
     that would exceed `budget` x the estimated time of one search of the
     real shape, candidates run on a prefix of the index columns sized to fit
-    the budget (the wave behaviour -- read tiles x splits against CTAs -- is
-    the real one; work units are shorter).  Results are cached per (rows,
+    the budget, and only splits and CTAs are tuned there (the wave behaviour
+    -- read tiles x splits against CTAs -- is the real one; work units are
+    shorter, which misleads the other knobs).  Results are cached per (rows,
     N, rdim, k, score) and, with `cache_path` (default $R2M_TUNE_CACHE),
     kept across runs."""
 
     RATE = 2.5e15  # FLOP/s: a model of the fused kernel, used only to size the budget
 
     def __init__(self, cache_path: str | None = None, reps: int = 1, proxy_cols: int = 0,
-                 budget: float = 0.15, min_proxy_tiles: int = 256):
+                 budget: float = 0.15, min_proxy_tiles: int = 256, min_gain: float = 0.02):
         import os
         self.reps = reps
+        self.min_gain = min_gain  # a candidate must beat the best by this fraction
         # > 0: force candidates onto the first proxy_cols index columns
         self.proxy_cols = proxy_cols
         self.budget = budget
@@ -145,19 +147,25 @@ class Autotuner:
             if cfg == best:
                 return
             ms = timed(cfg)
-            if ms < best_ms:
+            if ms < best_ms * (1.0 - self.min_gain):  # noise does not move the schedule
                 best, best_ms = cfg, ms
 
         for s, c in split_c[1:]:
             consider(splits=s, ctas=c)
-        consider(kernel="1sm" if rows > 128 else "2sm")
-        if eng.k <= 32:
-            consider(epilogue="4")
-            consider(epilogue="8")
-        consider(pace=32)
-        consider(pace=-1)
-        for kt in kt_c[1:]:
-            consider(kt=kt)
+        if target is eng:
+            # kernel, epilogue form, pacing and reservoir size depend on how
+            # long a work unit is and on how many pairs share an index tile
+            # in L2 -- a column prefix changes both, so these are tuned only on
+            # the real shape (on a 166K-column prefix the single-CTA kernel
+            # led by 3%, on the 20M-column index it ran 27% slower)
+            consider(kernel="1sm" if rows > 128 else "2sm")
+            if eng.k <= 32:
+                consider(epilogue="4")
+                consider(epilogue="8")
+            consider(pace=32)
+            consider(pace=-1)
+            for kt in kt_c[1:]:
+                consider(kt=kt)
         if target is not eng:
             target.close()
         self._apply(eng, best)

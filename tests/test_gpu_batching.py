@@ -62,17 +62,19 @@ def test_autotuner_keeps_results(setup, tmp_path):
     sub = reqs[:12]
     total = sum(w.shape[0] for w in sub)
     eng = rm.TopKEngine(idx.embeds8, k=20, rows_cap=rm.bucket_rows(total))
-    tuner = rm.Autotuner(str(tmp_path / "tune.json"))
+    # a generous budget: candidates run on the real engine, every knob is tried
+    tuner = rm.Autotuner(str(tmp_path / "tune.json"), budget=1e3)
     b = rm.RaggedBatcher(eng, re, total, tuner=tuner, use_graphs=True)
     got = b.run(sub)
     assert len(tuner.log) >= 6 and (tmp_path / "tune.json").exists()
+    assert all(e["cols"] == idx.N for e in tuner.log)
     assert {"kernel", "epilogue", "pace", "kt"} <= set(tuner.log[0])
     eng.set_tuning(0, 0, kernel="auto", epilogue="auto", pace=0, kt=0)
     ref = _per_request(eng, re, sub)
     for (v, l), (rv, rl) in zip(got, ref):
         assert np.array_equal(v, rv) and np.array_equal(l, rl)
     # a second tuner reads the persisted choice instead of timing again
-    t2 = rm.Autotuner(str(tmp_path / "tune.json"))
+    t2 = rm.Autotuner(str(tmp_path / "tune.json"), budget=1e3)
     b2 = rm.RaggedBatcher(eng, re, total, tuner=t2, use_graphs=True)
     got2 = b2.run(sub)
     assert t2.log == [] and t2.last.get("cached")
