@@ -40,6 +40,11 @@ KSTEP = 15
 Q = 65_536
 N_COLS = 16_777_216
 TOPK = 20
+# DRAM bytes (read + write) of one fused launch of 65,536 reads against
+# 2,097,152 index columns (ncu, small enough to capture); traffic grows with
+# the column count at a fixed read count, so the bench scales it by N
+SMALL_CASE_DRAM_BYTES = 17_415_128_576 + 34_015_232
+SMALL_CASE_COLS = 2_097_152
 ERR = 0.05
 TIE_F16 = 1e-3  # one fp16 step of a score near 1 (2^-10)
 GENOME_SEED, READ_SEED = 7, 11
@@ -882,10 +887,12 @@ def main():
                        "l2": "inputs > L2 (34 GB index streamed every step)"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": None,
+                         "traffic": SMALL_CASE_DRAM_BYTES * N / SMALL_CASE_COLS if nq == Q else None,
                          "traffic_algorithmic": nq * re.rdim + N * re.rdim,
-                         "traffic_note": "not measured in this run: DRAM bytes come from an ncu capture, "
-                                         "which a timed run cannot carry",
+                         "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                                         "65,536 reads x 2,097,152 columns (ncu, a 4.3 GB index) scaled by "
+                                         "the column count: the index is read once per wave of paced CTA "
+                                         "pairs, ~4x its size",
                          "kernel": ("k_gemm_topk2 (CTA-pair tcgen05 fp8 GEMM + fused top-20)" if nq > 128 else
                                     "k_gemm_topk (single-CTA tcgen05 fp8 GEMM + fused top-20)"),
                          "peak_basis": f"dense fp8 = 2 x {basis} sustained bf16 "
