@@ -452,11 +452,13 @@ HOST_READER_MAX_BYTES = 8 << 30  # inputs the host reader takes whole
 
 def pick_reader(file, reader: str = "auto") -> str:
     """reader = "auto": the native host reader when the host has >= 8 threads
-    and the input is at most 8 GiB (it parses the whole input at once; its
-    words then cross to the device at 40 bytes per 150 bp read, against ~190
-    bytes of FASTA for the GPU reader -- measured faster end to end, 5.9 vs
-    3.4 GB/s from host bytes), else the GPU reader, which streams any input
-    size through bounded memory."""
+    and the input is at most 8 GiB (it parses the whole input at once), else
+    the GPU reader, which streams any input size through bounded memory.
+    Parsing alone from host bytes the host reader is faster (6.3 vs 4.1
+    GB/s on 16 threads); in the whole run_map flow, where the host threads
+    also format the table, the GPU reader is (517K vs 459K reads/s, same
+    box), so "device" stays the default of the flows and "auto" is the
+    choice for hosts where parsing is the only host work."""
     if reader != "auto":
         return reader
     import os
@@ -474,11 +476,11 @@ def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int
                      batch_size: int = 8192, rows_cap: int | None = None, normalize: int = 0,
                      score: str = "f16", scaleB: torch.Tensor | None = None, parts: int | None = None,
                      segs: int | None = None, engine: TopKEngine | None = None, stream=None,
-                     reader: str = "auto", chunk_bytes: int = 1 << 30):
+                     reader: str = "device", chunk_bytes: int = 1 << 30):
     """rope_topk_stream (engine_fp8.jl:576-594): FASTA -> encode -> fp8 GEMM +
     top-k against the resident B -> TopKBatch per batch (file order).
 
-    reader = "auto" picks one of the two (pick_reader); "device" parses the FASTA on the GPU (the words stay in HBM),
+    reader = "device" (the default) parses the FASTA on the GPU (the words stay in HBM),
     `chunk_bytes` of the file at a time (cut at record starts), so inputs of
     any size stream through bounded memory; "host" uses the native host
     reader with `parts` threads on the whole input.  Both give the same
@@ -513,7 +515,7 @@ def resident_fits(host_bytes: int, rows_cap: int, rdim: int, k: int = 20, device
 def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size: int = 8192,
                              rows_cap: int | None = None, normalize: int = 0, score: str = "f16",
                              scaleB=None, resident: bool | None = None, chunk_cols: int = 1 << 20,
-                             depth: int = 3, pin: bool = True, reader: str = "auto", parts: int | None = None,
+                             depth: int = 3, pin: bool = True, reader: str = "device", parts: int | None = None,
                              stream=None, resident_chunks="auto"):
     """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index
     Bh (N, rdim) uint8.  resident = None applies resident_fits: an index that
