@@ -760,7 +760,10 @@ __host__ __device__ inline SparseLayout sparse_layout(int c, int m, int nslot, i
   L.smap = (ncm + 15) & ~15;
   L.acc = ((nslot * m * 8) + 15) & ~15;
   L.conv = ((nslot * m * outb) + 15) & ~15;
-  L.warp = L.smap + L.acc + 2 * L.conv;
+  // the two conversion arrays share their region with the per-c-mer group
+  // masks of the accumulation (4 bytes per c-mer), which they follow
+  const int masks = (4 * ncm + 15) & ~15;
+  L.warp = L.smap + L.acc + (2 * L.conv > masks ? 2 * L.conv : masks);
   return L;
 }
 
@@ -815,7 +818,12 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   const unsigned FULL = 0xFFFFFFFFu;
   const unsigned lt = (1u << lane) - 1u;
   const int ncm = 1 << (2 * P.c);
+  // group masks of the accumulation: bit l of gmask[cb] = lane l's window
+  // has c-mer cb (formed with shared atomic ORs, cleared by each group's
+  // leader after its batch, so zero between batches)
+  uint32_t *gmask = reinterpret_cast<uint32_t *>(conv_re);
   for (int i = lane * 16; i < ncm; i += 512) *reinterpret_cast<uint4 *>(smap + i) = make_uint4(~0u, ~0u, ~0u, ~0u);
+  for (int i = lane * 4; i < ncm; i += 128) *reinterpret_cast<uint4 *>(gmask + i) = make_uint4(0u, 0u, 0u, 0u);
   __syncwarp();
   // ---- accumulate, window order
   int nslots = 0;
@@ -828,7 +836,11 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
     const uint32_t smer = v & P.bmask;
     const uint32_t upper = (2 * P.c >= 32) ? 0u : (smer >> (2 * P.c));
     const uint32_t cb = (smer & P.cbmask) ^ ((upper * 0x9E3779B1u) & P.cbmask);
-    const unsigned grp = __match_any_sync(FULL, valid ? cb : (0x40000000u | (uint32_t)lane));
+    // the lanes of this batch whose windows share a c-mer (a group), as a
+    // lane mask: every lane ORs its bit into its c-mer's word
+    if (valid) atomicOr(gmask + cb, 1u << lane);
+    __syncwarp();
+    const unsigned grp = valid ? gmask[cb] : (1u << lane);
     const int rank = __popc(grp & lt);
     const bool leader = valid && rank == 0;
     int s_l = 0xFF;
@@ -841,6 +853,7 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
     }
     nslots += __popc(newm);
     const int slot = __shfl_sync(FULL, s_l, __ffs(grp) - 1);
+    if (leader) gmask[cb] = 0u;  // read by all members above; the rounds below end with a warp sync
     float2 ph[M];
     if (valid) ld_planes<M>(table, P.nw, p, ph);
     const int rounds = (int)__reduce_max_sync(FULL, valid ? (unsigned)rank : 0u);
