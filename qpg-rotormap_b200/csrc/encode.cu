@@ -781,7 +781,7 @@ __device__ __forceinline__ void ld_planes(const float2 *base, int stride, int i,
     const float4 *b4 = reinterpret_cast<const float4 *>(base);
 #pragma unroll
     for (int j = 0; j < M / 2; ++j) {
-      const float4 t = b4[(size_t)j * stride + i];
+      const float4 t = b4[j * stride + i];
       v[2 * j] = make_float2(t.x, t.y);
       v[2 * j + 1] = make_float2(t.z, t.w);
     }
@@ -795,7 +795,7 @@ __device__ __forceinline__ void st_planes(float2 *base, int stride, int i, const
     float4 *b4 = reinterpret_cast<float4 *>(base);
 #pragma unroll
     for (int j = 0; j < M / 2; ++j)
-      b4[(size_t)j * stride + i] = make_float4(v[2 * j].x, v[2 * j].y, v[2 * j + 1].x, v[2 * j + 1].y);
+      b4[j * stride + i] = make_float4(v[2 * j].x, v[2 * j].y, v[2 * j + 1].x, v[2 * j + 1].y);
   }
 }
 
@@ -827,15 +827,17 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   __syncwarp();
   // ---- accumulate, window order
   int nslots = 0;
-  for (int b0 = 0; b0 < P.nw; b0 += 32) {
+  const int nw = P.nw;
+  const uint32_t bmask = P.bmask, cbmask = P.cbmask, c2 = 2u * (uint32_t)P.c;
+  for (int b0 = 0; b0 < nw; b0 += 32) {
     const int p = b0 + lane;
-    const bool valid = p < P.nw;
+    const bool valid = p < nw;
     const int wo = p >> 4;
     const uint32_t w0 = __shfl_sync(FULL, wreg, wo & 31), w1 = __shfl_sync(FULL, wreg, (wo + 1) & 31);
     const uint32_t v = __funnelshift_r(w0, w1, (uint32_t)(p & 15) << 1);
-    const uint32_t smer = v & P.bmask;
-    const uint32_t upper = (2 * P.c >= 32) ? 0u : (smer >> (2 * P.c));
-    const uint32_t cb = (smer & P.cbmask) ^ ((upper * 0x9E3779B1u) & P.cbmask);
+    const uint32_t smer = v & bmask;
+    const uint32_t upper = c2 >= 32u ? 0u : (smer >> c2);
+    const uint32_t cb = (smer & cbmask) ^ ((upper * 0x9E3779B1u) & cbmask);
     // the lanes of this batch whose windows share a c-mer (a group), as a
     // lane mask: every lane ORs its bit into its c-mer's word
     if (valid) atomicOr(gmask + cb, 1u << lane);
@@ -855,22 +857,35 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
     const int slot = __shfl_sync(FULL, s_l, __ffs(grp) - 1);
     if (leader) gmask[cb] = 0u;  // read by all members above; the rounds below end with a warp sync
     float2 ph[M];
-    if (valid) ld_planes<M>(table, P.nw, p, ph);
-    const int rounds = (int)__reduce_max_sync(FULL, valid ? (unsigned)rank : 0u);
-    for (int r = 0; r <= rounds; ++r) {
-      if (valid && rank == r) {
-        float2 a[M];
-        if (r == 0 && isnew) {
+    if (valid) ld_planes<M>(table, nw, p, ph);
+    // round 0: every group's first member (distinct slots: no conflict)
+    if (leader) {
+      float2 a[M];
+      if (isnew) {
 #pragma unroll
-          for (int q = 0; q < M; ++q) a[q] = make_float2(0.f, 0.f);  // 0 + x, as a cleared bin
-        } else {
-          ld_planes<M>(acc, ns, slot, a);
-        }
-#pragma unroll
-        for (int q = 0; q < M; ++q) a[q] = add2(a[q], ph[q]);
-        st_planes<M>(acc, ns, slot, a);
+        for (int q = 0; q < M; ++q) a[q] = make_float2(0.f, 0.f);  // 0 + x, as a cleared bin
+      } else {
+        ld_planes<M>(acc, ns, slot, a);
       }
-      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < M; ++q) a[q] = add2(a[q], ph[q]);
+      st_planes<M>(acc, ns, slot, a);
+    }
+    __syncwarp();
+    // later rounds: the r-th member of every group with more than r members
+    const unsigned more = __ballot_sync(FULL, valid && rank > 0);
+    if (more) {
+      const int rounds = (int)__reduce_max_sync(FULL, valid ? (unsigned)rank : 0u);
+      for (int r = 1; r <= rounds; ++r) {
+        if (valid && rank == r) {
+          float2 a[M];
+          ld_planes<M>(acc, ns, slot, a);
+#pragma unroll
+          for (int q = 0; q < M; ++q) a[q] = add2(a[q], ph[q]);
+          st_planes<M>(acc, ns, slot, a);
+        }
+        __syncwarp();
+      }
     }
   }
   // ---- the G-homopolymer c-mer's bins are zero
@@ -886,18 +901,21 @@ __device__ __forceinline__ void sparse_fragment(const EncParams &P, const float2
   __syncwarp();
   // ---- per-copy energies and the largest magnitude
   float part[M], mx = 0.f;
+  float2 e2[M];  // per copy: sum of Re^2 and sum of Im^2, paired
 #pragma unroll
-  for (int q = 0; q < M; ++q) part[q] = 0.f;
+  for (int q = 0; q < M; ++q) e2[q] = make_float2(0.f, 0.f);
   for (int sl = lane; sl < nslots; sl += 32) {
     float2 zv[M];
     ld_planes<M>(acc, ns, sl, zv);
 #pragma unroll
     for (int q = 0; q < M; ++q) {
       const float2 z = zv[q];
-      part[q] += __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
+      e2[q] = fma2(z, z, e2[q]);
       mx = fmaxf(mx, fmaxf(fabsf(z.x), fabsf(z.y)));
     }
   }
+#pragma unroll
+  for (int q = 0; q < M; ++q) part[q] = e2[q].x + e2[q].y;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
