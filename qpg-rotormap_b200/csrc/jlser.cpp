@@ -48,6 +48,7 @@
 #include <unistd.h>
 
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -311,6 +312,7 @@ struct Reader {
 
   JP tuple(size_t n) {
     JP o = mk(JObj::TUPLE);
+    need(n);  // every element takes at least one byte
     o->items.reserve(n);
     for (size_t i = 0; i < n; ++i) o->items.push_back(obj());
     return o;
@@ -383,11 +385,11 @@ struct Reader {
     size_t n = 1;
     for (int64_t d : arr->dims) {
       if (d < 0) throw ParseError{"negative array dimension"};
-      n *= (size_t)d;
+      if (__builtin_mul_overflow(n, (size_t)d, &n)) throw ParseError{"array dimensions overflow"};
     }
     const int es = elem_size(*arr->elty);
     if (es > 0) {
-      arr->nbytes = n * (size_t)es;
+      if (__builtin_mul_overflow(n, (size_t)es, &arr->nbytes)) throw ParseError{"array size overflows"};
       need(arr->nbytes);
       arr->data = p;
       p += arr->nbytes;
@@ -401,6 +403,7 @@ struct Reader {
 
   // Vector{String} elements, the one hot loop (a column count of entries).
   void string_elements(JObj &arr, size_t n) {
+    need(n);  // every element takes at least one byte
     arr.sidx.resize(n);
     std::unordered_map<std::string, int32_t> inline_ids;
     auto intern_obj = [&](JObj *s) -> int32_t {
@@ -498,6 +501,8 @@ static int jlbin_parse(r2m_jlbin *h, const uint8_t *data, size_t len) {
     return r2m::fail(R2M_EIO, "index .bin: " + e.msg);
   } catch (const std::bad_alloc &) {
     return r2m::fail(R2M_ENOMEM, "index .bin: out of host memory");
+  } catch (const std::exception &e) {
+    return r2m::fail(R2M_EIO, std::string("index .bin: ") + e.what());
   }
   h->base = data;
   const size_t nf = h->nt->items.size();

@@ -244,6 +244,16 @@ struct r2m_server {
       if (e != cudaSuccess) {
         cudaGetLastError();
         r->d_mem = nullptr;
+        if (active.empty() && inflight.empty() && downloads.empty()) {
+          // nothing will free memory: fail it rather than wait forever
+          r->state = R2M_REQ_FAILED;
+          r->error = std::string("device allocation for the request failed: ") + cudaGetErrorString(e);
+          r->t_done = now_s();
+          st.requests_failed++;
+          done_cv.notify_all();
+          any = true;
+          continue;
+        }
         waiting.push_front(r);
         break;  // try again when memory frees up
       }

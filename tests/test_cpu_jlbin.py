@@ -215,3 +215,19 @@ def test_attach_genome_from_source(tmp_path):
     idx.k, idx.genome, idx.col_pos = 50, None, None
     rm.attach_genome(idx)
     assert np.array_equal(idx.col_pos, np.concatenate([pos, pos])) and np.array_equal(idx.genome, pack.words)
+
+
+@pytest.mark.parametrize("body", [
+    bytes([45]) + struct.pack("<i", 2_000_000_000),                        # LONGTUPLE of 2e9 items
+    bytes([21, 0, 8, 20, 2, 49]) + struct.pack("<i", 2**30) + bytes([49]) + struct.pack("<i", 2**30),  # Int64 2^30 x 2^30
+    bytes([21, 0, 33, 8]) + struct.pack("<q", 2**62),                       # String vector of 2^62
+    bytes([21, 0, 13, 8]) + struct.pack("<q", 2**61),                       # Float32 vector: size overflows
+    bytes([48]) + struct.pack("<i", -5),                                    # negative string length
+])
+def test_hostile_sizes_are_refused_not_trusted(tmp_path, body):
+    """Counts and dims far beyond the stream's length fail with a parse
+    error before any allocation or read trusts them."""
+    p = tmp_path / "h.bin"
+    p.write_bytes(bytes([55]) + b"JL" + bytes([20, 4, 0, 0, 0]) + body)
+    with pytest.raises(R2MError, match="index .bin"):
+        jlbin.read_bin(p)
