@@ -205,10 +205,33 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def fp64_check(re, idx, genome_dev, words_dev, locs8, vals8, n_sample: int, seed: int):
+    """Top-20 recall and score error of the fp8 search against the exact
+    FP64 search over all index columns (the GPU check kernel, windows
+    re-encoded with the golden fp64 encoder) on `n_sample` sampled reads."""
+    import torch
+    import rotormap as rm
+    rng = np.random.default_rng(seed)
+    nq = words_dev.shape[0]
+    samp = np.sort(rng.choice(nq, size=min(n_sample, nq), replace=False))
+    ds = torch.from_numpy(samp).to(words_dev.device)
+    meta = rm.DeviceMeta(idx, genome=genome_dev)
+    cand = locs8[ds].contiguous()
+    t0 = time.perf_counter()
+    v64, l64, c64 = rm.check_fp64(re, meta, words_dev[ds].contiguous(), cand)
+    secs = time.perf_counter() - t0
+    l8, l64, v8, c64 = cand.cpu().numpy(), l64.cpu().numpy(), vals8[ds].cpu().numpy(), c64.cpu().numpy()
+    rec = float(np.mean([len(set(a) & set(b)) / TOPK for a, b in zip(l8, l64)]))
+    err = np.abs(v8.astype(np.float64) - c64)
+    del meta
+    return {"sampled_rows": int(samp.size), "seconds": secs, "top20_recall_fp8_vs_fp64": rec,
+            "score_abs_err_fp8": {"max": float(err.max()), "mean": float(err.mean())}}
+
+
 # ---------------------------------------------------------------- serving leg
 
 
-def serving_leg(dev, n_requests: int = 16, seed: int = 31):
+def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0):
     """Serving form vs the plain batch path at human-scale geometry: 3.1 Gbp
     genome of 24 records (lengths U[50, 250] Mbp rescaled, GC 41%, 5% N runs),
     fwd + rc windows at k = 150, kstep = 1880 -> ~3.3M columns (~6.3 GiB e4m3),
@@ -230,7 +253,6 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31):
         recs, offs = synth.sample_positions(nbases, runs, int(n), K_BASES, seed + 10 + i)
         reqs.append(synth.extract_reads_packed(words, woff, recs, offs, K_BASES, float(errs[i]), seed + 10 + i))
         truth.append((recs, offs))
-    del words
     torch.cuda.empty_cache()
     total = int(sizes.sum())
     # arrivals: Poisson, mean gap = mean request / (1.5 x a fused-kernel capacity estimate)
@@ -312,7 +334,13 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31):
         ok = (recmap[c] == recs[:, None]) & (np.abs(idx.starts[c] - (offs[:, None] + 1)) < K_BASES)
         hit += int(ok.any(axis=1).sum())
     out["mapped_frac_top20"] = hit / total
-    del idx
+    if fp64_sample > 0:
+        W = re.words
+        allw = torch.from_numpy(np.concatenate(reqs).reshape(-1).view(np.int32)).to(dev).view(-1, W)
+        out["fp64_check"] = fp64_check(re, idx, words, allw, torch.from_numpy(sl).to(dev),
+                                       torch.from_numpy(sv).to(dev), fp64_sample, seed + 5)
+        del allw
+    del idx, words
     torch.cuda.empty_cache()
     return out
 
@@ -713,6 +741,9 @@ def summary(line: dict) -> dict:
            "gemm_tflops": _r(line["roofline"]["achieved"]), "gemm_frac_of_2x_bf16": _r(line["roofline"]["frac"], 3),
            "encoder_gbs": _r(line["encoder"]["achieved_gbs"]),
            "encoder_frac_hbm": _r(line["encoder"]["achieved_gbs"] / line["encoder"]["peak_gbs"], 3)}
+    if line.get("fp64_check"):
+        out["C1_fp64_recall"] = _r(line["fp64_check"]["top20_recall_fp8_vs_fp64"], 4)
+        out["C1_fp64_err_max"] = _r(line["fp64_check"]["score_abs_err_fp8"]["max"], 3)
     if "tensor_pipe" in line["roofline"]:
         out["tensor_pipe_est"] = _r(line["roofline"]["tensor_pipe"].get("est_active_frac"), 3)
     sv = line.get("serving")
@@ -724,6 +755,9 @@ def summary(line: dict) -> dict:
                                                          sv["plain_fused_kernel"]["reads_per_s"], 3),
                              "recall_vs_plain_ties": _r(sv["top20_recall_vs_plain_reference"], 6),
                              "untied_misses": sv["untied_misses"], "reads": sv["reads"]}
+        if sv.get("fp64_check"):
+            out["C4_serving"]["fp64_recall"] = _r(sv["fp64_check"]["top20_recall_fp8_vs_fp64"], 4)
+            out["C4_serving"]["fp64_err_max"] = _r(sv["fp64_check"]["score_abs_err_fp8"]["max"], 3)
     pr = line.get("precision")
     if pr:
         fc = pr["fp64_check"]
@@ -772,6 +806,8 @@ def main():
     ap.add_argument("--batching-requests", type=int, default=256)
     ap.add_argument("--precision-reads", type=int, default=1_000_000)
     ap.add_argument("--precision-sample", type=int, default=10_000)
+    ap.add_argument("--fp64-sample", type=int, default=1000,
+                    help="reads of the headline and serving legs checked against the exact FP64 search")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -845,6 +881,11 @@ def main():
     from rotormap._lib import check, lib
     check(lib().r2m_check_device_error(None))
     frac = mapped_fraction(d_loc.cpu().numpy(), starts0, idx.starts)
+    fp64 = None
+    if rank == 0 and args.fp64_sample > 0:
+        g_dev = torch.from_numpy(pack.words.view(np.int32)).to(dev)
+        fp64 = fp64_check(re, idx, g_dev, d_words.view(nq, re.words), d_loc, d_val, args.fp64_sample, 13)
+        del g_dev
 
     # end to end through the public API with host buffers
     mapper = rm.Mapper(eng, re)
@@ -909,6 +950,7 @@ def main():
                            "encode": sum(enc_ms) / len(enc_ms)},
             "index_build_s": t_index,
             "mapped_frac_top20": frac,
+            "fp64_check": fp64,
             "e2e": {"value": nq * world / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": mapper.h2d_bytes(nq),
                     "d2h_bytes_per_step": mapper.d2h_bytes(nq)},
             "gpu_launches": 3 * args.steps,
@@ -921,7 +963,7 @@ def main():
     torch.cuda.empty_cache()
     if rank == 0:
         if world == 1 and not args.no_serving:
-            line["serving"] = serving_leg(dev, args.requests)
+            line["serving"] = serving_leg(dev, args.requests, fp64_sample=args.fp64_sample)
         if world == 1 and not args.no_precision:
             line["precision"] = precision_leg(dev, args.precision_reads, args.precision_sample)
         if world == 1 and not args.no_batching:
