@@ -451,14 +451,14 @@ HOST_READER_MAX_BYTES = 8 << 30  # inputs the host reader takes whole
 
 
 def pick_reader(file, reader: str = "auto") -> str:
-    """reader = "auto": the native host reader when the host has >= 8 threads
-    and the input is at most 8 GiB (it parses the whole input at once), else
-    the GPU reader, which streams any input size through bounded memory.
-    Parsing alone from host bytes the host reader is faster (6.3 vs 4.1
-    GB/s on 16 threads); in the whole run_map flow, where the host threads
-    also format the table, the GPU reader is (517K vs 459K reads/s, same
-    box), so "device" stays the default of the flows and "auto" is the
-    choice for hosts where parsing is the only host work."""
+    """reader = "auto" (the flows' default): the native host reader when the
+    host has >= 8 threads and the input is at most 8 GiB (it parses the
+    whole input at once), else the GPU reader, which streams any input size
+    through bounded memory.  Parsing alone from host bytes the host reader
+    is faster (6.3 vs 3.9 GB/s on 16 threads); in the whole run_map flow,
+    where host threads also format the table, the two are within a few
+    percent of each other (514K vs 512K reads/s in one run, 459K vs 517K in
+    another, same box)."""
     if reader != "auto":
         return reader
     import os
@@ -467,7 +467,7 @@ def pick_reader(file, reader: str = "auto") -> str:
     else:
         try:
             size = os.path.getsize(file)
-        except OSError:
+        except (OSError, TypeError):
             return "device"
     return "host" if (os.cpu_count() or 1) >= 8 and size <= HOST_READER_MAX_BYTES else "device"
 
@@ -476,7 +476,7 @@ def rope_topk_stream(re: RopeEncoder, file, B: torch.Tensor, k: int = 20, w: int
                      batch_size: int = 8192, rows_cap: int | None = None, normalize: int = 0,
                      score: str = "f16", scaleB: torch.Tensor | None = None, parts: int | None = None,
                      segs: int | None = None, engine: TopKEngine | None = None, stream=None,
-                     reader: str = "device", chunk_bytes: int = 1 << 30):
+                     reader: str = "auto", chunk_bytes: int = 1 << 30):
     """rope_topk_stream (engine_fp8.jl:576-594): FASTA -> encode -> fp8 GEMM +
     top-k against the resident B -> TopKBatch per batch (file order).
 
@@ -515,7 +515,7 @@ def resident_fits(host_bytes: int, rows_cap: int, rdim: int, k: int = 20, device
 def rope_topk_stream_compact(re: RopeEncoder, file, Bh, k: int = 20, batch_size: int = 8192,
                              rows_cap: int | None = None, normalize: int = 0, score: str = "f16",
                              scaleB=None, resident: bool | None = None, chunk_cols: int = 1 << 20,
-                             depth: int = 3, pin: bool = True, reader: str = "device", parts: int | None = None,
+                             depth: int = 3, pin: bool = True, reader: str = "auto", parts: int | None = None,
                              stream=None, resident_chunks="auto"):
     """rope_topk_stream_compact (engine_compact.jl:415-457) with a host index
     Bh (N, rdim) uint8.  resident = None applies resident_fits: an index that

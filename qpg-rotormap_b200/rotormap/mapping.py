@@ -121,7 +121,7 @@ def julia_repr_f32(x: float) -> str:
 
 
 def run_map(index, reads, out=None, topk: int = 20, batch_size: int = 8192, verbose: bool = False,
-            score: str | None = None, reader: str = "device") -> int:
+            score: str | None = None, reader: str = "auto") -> int:
     """run_map (map.jl:100-184): INDEX + READS -> the match table at `out`
     (default READS + ".maps").  Returns the number of reads mapped.
 
