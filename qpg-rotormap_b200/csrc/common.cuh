@@ -305,4 +305,14 @@ __device__ __forceinline__ void mma_commit_pair(uint32_t bar_cluster) {
   asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_cluster)
                : "memory");
 }
+// The same arrive on the barrier at shared::cta offset `bar_cta` of every CTA
+// in `cta_mask`: one commit releases a stage in both CTAs of a pair.  This
+// is the commit's own arrive-multicast, not a load: no data moves.
+__device__ __forceinline__ void mma_commit_pair_mask(uint32_t bar_cta, uint16_t cta_mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          bar_cta),
+      "h"(cta_mask)
+      : "memory");
+}
 }  // namespace r2m

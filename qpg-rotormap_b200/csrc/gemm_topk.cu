@@ -47,11 +47,14 @@ constexpr int MAX_SPLITS = 128;
 // share each TMEM lane quarter, each draining one half (128 columns) of
 // every tile into its own reservoir, so a (read tile, column split) unit
 // leaves two partial lists per row.  That halves the per-warp latency chain
-// of a tile and the reservoir warm-up at every unit start -- the gain of short
-// units -- but keeps more warps busy, which under the board's power cap
-// lowers the clock of long units; the host picks H per launch
-// (epi_halves_for).  KT = 64 always uses H = 1 (its reservoir needs the
-// registers).
+// of a tile and the reservoir warm-up at every unit start.  The CTA-pair
+// kernel always takes it (k <= 32): its epilogue must drain a tile in the
+// time its MMAs take one, and with 4 warps it held the MMAs back (headline
+// launch, same box: 1,553 ms per launch with 4 epilogue warps, 1,530 ms with
+// 8).  The single-CTA kernel takes it for short units only: on long units
+// the extra warps cost clock under the board's power cap.  The host picks H
+// per launch (epi_halves_for).  KT = 64 always uses H = 1 (its reservoir
+// needs the registers).
 __host__ __device__ constexpr int epi_threads(int H) { return 64 + 128 * H; }
 constexpr int SCRATCH_F = 17;  // floats per epilogue thread (16-value slow-path passes)
 // 256-column tiles per work unit at or below which the 8-warp epilogue pays
@@ -464,15 +467,30 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
 // 2-SM variant: a CTA pair (cluster of 2) computes a 256-read x 256-column
 // tile with tcgen05.mma.cta_group::2 (M = 256, N = 256, K = 32).  Each CTA
 // loads its own 128 read rows and its own 128 of the 256 index columns per
-// stage (32 KiB instead of 48 KiB per CTA), so a CTA pulls 2/3 of the
+// K chunk (32 KiB instead of 48 KiB per CTA), so a CTA pulls 2/3 of the
 // single-CTA kernel's operand bytes per FLOP.  The leader CTA (rank 0)
 // issues the MMAs; both CTAs' TMA loads complete on the leader's stage
 // barrier; the leader's commits release both CTAs' stages and signal both
 // CTAs' accumulators; each CTA's epilogue drains its own 128 TMEM lanes (all
 // 256 columns) and arrives on the leader's accumulator-empty barrier.  No
-// multicast is used anywhere.
-constexpr int STAGES2 = 6;
-constexpr int HALF_TILE = 128 * BK;  // 16 KiB
+// load uses multicast.
+//
+// A stage holds two 128-byte K chunks (8 MMAs), and one commit releases it in
+// both CTAs (the commit's arrive goes to the barrier at the same offset in
+// each CTA of the mask).  The one issuing thread is what bounds this kernel:
+// per stage it waits on the stage barrier, forms descriptors, issues the
+// MMAs and commits.  With one chunk and two commits per stage that took ~730
+// SM clocks against 512 of tensor work (clock64 probes on the headline
+// launch, 65,536 reads x 16.8M columns), so the tensor pipe idled ~30% of the
+// time.  Same-box A/B, identical results: 1,697 ms per launch -> 1,553 ms
+// with two chunks per stage, one commit and precomputed descriptors; three
+// chunks per stage (two stages in flight) 1,800 ms; one commit to the leader
+// passed on to the peer by the leader's producer (the peer's loads then
+// start later) 1,983 ms.
+constexpr int HALF_TILE = 128 * BK;            // 16 KiB: one 128-byte K chunk of 128 rows
+constexpr int KCH = 2;                         // K chunks per stage
+constexpr int STAGES2 = 3;                     // stages in flight (3 x 64 KiB per CTA)
+constexpr int STAGE2_BYTES = KCH * HALF_TILE;  // per operand and CTA
 
 // Pair pacing.  Every pair streams the index in column order, and the pairs
 // of one wave (units p, p + npairs, ... run side by side) read the same index
@@ -519,8 +537,8 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
   unsigned char *smem =
       reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t *sA = smem;
-  uint8_t *sB = smem + STAGES2 * HALF_TILE;
-  uint64_t *full = reinterpret_cast<uint64_t *>(sB + STAGES2 * HALF_TILE);
+  uint8_t *sB = smem + STAGES2 * STAGE2_BYTES;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sB + STAGES2 * STAGE2_BYTES);
   uint64_t *empty = full + STAGES2;
   uint64_t *acc_full = empty + STAGES2;
   uint64_t *acc_empty = acc_full + 2;
@@ -577,7 +595,7 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
         const int t0 = split_lo(sp, g.n_tiles, g.splits), t1 = split_lo(sp + 1, g.n_tiles, g.splits);
         for (int t = t0; ok && t < t1; ++t) {
           if (pacing && (t - t0) % PACE_EVERY == 0) pace_pair(g.pace, pair, npairs, pos + (t - t0), g.pace_window);
-          for (int kb = 0; kb < g.num_kb; ++kb) {
+          for (int kb = 0; kb < g.num_kb; kb += KCH) {
             if (!mbar_wait_bounded(&empty[stage], phase ^ 1u, abort_flag, WAIT_LIMIT)) {
               if (!*abort_flag) atomicExch(g.err, kErrTimeoutEmpty);
               *abort_flag = 1;
@@ -585,9 +603,14 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
               break;
             }
             const uint32_t fbar = mapa_shared(smem_u32(&full[stage]), 0);
-            if (leader) mbar_arrive_expect_tx(&full[stage], 4 * HALF_TILE);
-            tma_load_2d_pair(sA + stage * HALF_TILE, &tmA, fbar, kb * BK, mt * 256 + (int)rank * 128);
-            tma_load_2d_pair(sB + stage * HALF_TILE, &tmB, fbar, kb * BK, t * BN + (int)rank * 128);
+            const int nch = g.num_kb - kb < KCH ? g.num_kb - kb : KCH;
+            if (leader) mbar_arrive_expect_tx(&full[stage], 4 * HALF_TILE * nch);
+            for (int c = 0; c < nch; ++c) {
+              tma_load_2d_pair(sA + stage * STAGE2_BYTES + c * HALF_TILE, &tmA, fbar, (kb + c) * BK,
+                               mt * 256 + (int)rank * 128);
+              tma_load_2d_pair(sB + stage * STAGE2_BYTES + c * HALF_TILE, &tmB, fbar, (kb + c) * BK,
+                               t * BN + (int)rank * 128);
+            }
             ++issued;
             if (++stage == STAGES2) {
               stage = 0;
@@ -618,6 +641,9 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
     // ------------------------------------------------ MMA issuer (leader CTA)
     if (lane == 0 && leader) {
       const uint32_t idesc = idesc_e4m3_f32(256, BN);
+      // descriptors of stage 0; a stage / chunk / K step offset adds its
+      // 16-byte units to the start-address field
+      const uint64_t dA0 = smem_desc_sw128(smem_u32(sA)), dB0 = smem_desc_sw128(smem_u32(sB));
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
@@ -635,7 +661,7 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
           }
           tc_fence_after();
           const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-          for (int kb = 0; kb < g.num_kb; ++kb) {
+          for (int kb = 0; kb < g.num_kb; kb += KCH) {
             if (!mbar_wait_bounded(&full[stage], phase, abort_flag, WAIT_LIMIT)) {
               if (!*abort_flag) atomicExch(g.err, kErrTimeoutFull);
               *abort_flag = 1;
@@ -643,15 +669,19 @@ __global__ void __launch_bounds__(epi_threads(H), 1)
               break;
             }
             tc_fence_after();
-            const uint32_t a0 = smem_u32(sA + stage * HALF_TILE);
-            const uint32_t b0 = smem_u32(sB + stage * HALF_TILE);
+            const int nch = g.num_kb - kb < KCH ? g.num_kb - kb : KCH;
+            const uint64_t so = (uint64_t)((stage * STAGE2_BYTES) >> 4);
 #pragma unroll
-            for (int kk = 0; kk < BK / 32; ++kk)
-              mma_f8_pair(d_tmem, smem_desc_sw128(a0 + kk * 32), smem_desc_sw128(b0 + kk * 32), idesc,
-                          (kb | kk) != 0 ? 1u : 0u);
-            const uint32_t eb = smem_u32(&empty[stage]);
-            mma_commit_pair(mapa_shared(eb, 0));
-            mma_commit_pair(mapa_shared(eb, 1));
+            for (int c = 0; c < KCH; ++c) {
+              if (c < nch) {
+#pragma unroll
+                for (int kk = 0; kk < BK / 32; ++kk) {
+                  const uint64_t o = so + (uint64_t)((c * HALF_TILE + kk * 32) >> 4);
+                  mma_f8_pair(d_tmem, dA0 + o, dB0 + o, idesc, ((kb + c) | kk) != 0 ? 1u : 0u);
+                }
+              }
+            }
+            mma_commit_pair_mask(smem_u32(&empty[stage]), (uint16_t)3);  // both CTAs' stage
             if (++stage == STAGES2) {
               stage = 0;
               phase ^= 1u;
@@ -897,13 +927,17 @@ static int launch_gemm(const CUtensorMap &mA, const CUtensorMap &mB, const GemmA
 }
 
 static size_t gemm2_smem_bytes(int H) {
-  return 1024 + (size_t)STAGES2 * 2 * HALF_TILE + (2 * STAGES2 + 5) * 8 + 16 +
+  return 1024 + (size_t)STAGES2 * 2 * STAGE2_BYTES + (2 * STAGES2 + 5) * 8 + 16 +
          (size_t)(epi_threads(H) - 64) * SCRATCH_F * sizeof(float);
 }
 
-// Epilogue halves for a pair-kernel launch: 2 for short units (k <= 32).
-static int epi_halves_for(int KT, int n_tiles, int splits) {
-  return (KT <= 32 && (n_tiles + splits - 1) / splits <= SHORT_UNIT_TILES) ? 2 : 1;
+// Epilogue halves of a launch of kernel `kind`: the CTA-pair kernel always
+// takes 2 when the reservoir allows (k <= 32), the single-CTA kernel for
+// short units only.
+static int epi_halves_for(int kind, int KT, int n_tiles, int splits) {
+  if (KT > 32) return 1;
+  if (kind == 2) return 2;
+  return (n_tiles + splits - 1) / splits <= SHORT_UNIT_TILES ? 2 : 1;
 }
 
 template <int KT, int H>
@@ -1254,7 +1288,7 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   const int hmax = eng->KT <= 32 ? 2 : 1;
   g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / hmax);
   const int halves =
-      eng->epi == 1 ? 1 : eng->epi == 2 ? hmax : epi_halves_for(eng->KT, eng->n_tiles, g.splits);
+      eng->epi == 1 ? 1 : eng->epi == 2 ? hmax : epi_halves_for(kind, eng->KT, eng->n_tiles, g.splits);
   const int lists_per_row = halves * g.splits;  // partial lists each row leaves
   g.num_kb = (eng->rdim + BK - 1) / BK;
   g.score_mode = eng->score_mode;
@@ -1436,10 +1470,10 @@ extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_sc
   const int hmax = KT <= 32 ? 2 : 1;
   // the engine's automatic schedule, with the splits cut to the scratch
   int splits = choose_splits(m_tiles, n_tiles, ctas_eff, 0, MAX_SPLITS / hmax);
-  int halves = epi_halves_for(KT, n_tiles, splits);
+  int halves = epi_halves_for(kind, KT, n_tiles, splits);
   while (splits > 1 && (size_t)halves * splits * mpad > max_lists) {
     --splits;
-    halves = epi_halves_for(KT, n_tiles, splits);
+    halves = epi_halves_for(kind, KT, n_tiles, splits);
   }
   if ((size_t)halves * splits * mpad > max_lists) halves = 1;
   GemmArgs g;
