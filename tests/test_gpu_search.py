@@ -227,3 +227,27 @@ def test_pair_pacing_changes_only_the_schedule(epilogue, score):
     rv, rl = orc.topk_e4m3(A8, B8, 20, 2 if score == "scaled" else 0, sa, sb)
     for v, l in outs:
         assert np.array_equal(v, rv) and np.array_equal(l, rl)
+
+
+@pytest.mark.parametrize("nb,N", [(300, 70001), (64, 1000), (257, 4133)])
+@pytest.mark.parametrize("k", [20, 32, 64])
+@pytest.mark.parametrize("kernel", ["1sm", "2sm"])
+def test_scaled_scores_exact_with_zero_and_negative_scales(nb, N, k, kernel):
+    """Scaled scores with power-of-two row and column scales are exact, so
+    the lists must equal the oracle's bit for bit, ties included, with zero
+    column scales, negative column scales, a 32-column run of zero scales and
+    a ragged last tile; k = 32 and 64 take the one-chunk-at-a-time and the
+    64-entry reservoir epilogues."""
+    rng = np.random.default_rng(nb + 3 * N + k)
+    rdim = 256
+    A8, _ = int_e4m3(rng, (nb, rdim), -2, 2)
+    B8, _ = int_e4m3(rng, (N, rdim), -2, 2)
+    sa = rng.choice(np.array([0.5, 1.0, 2.0], np.float32), nb)
+    sb = rng.choice(np.array([0.25, 0.5, 1.0, 2.0, 4.0], np.float32), N)
+    sb[rng.random(N) < 0.05] = 0.0
+    sb[rng.random(N) < 0.02] *= -1.0
+    sb[64:96] = 0.0  # one chunk of zero scales
+    v, l = run_engine(A8, B8, k, "scaled", scaleA=sa, scaleB=sb, kernel=kernel)
+    ov, ol = orc.topk_e4m3(A8, B8, k, 2, sa, sb)
+    assert np.array_equal(v, ov)
+    assert np.array_equal(l, ol)
