@@ -43,7 +43,7 @@ TOPK = 20
 # DRAM bytes (read + write) of one fused launch of 65,536 reads against
 # 2,097,152 index columns (ncu, small enough to capture); traffic grows with
 # the column count at a fixed read count, so the bench scales it by N
-SMALL_CASE_DRAM_BYTES = 17_415_128_576 + 34_015_232
+SMALL_CASE_DRAM_BYTES = 17_403_048_448 + 30_679_040
 SMALL_CASE_COLS = 2_097_152
 ERR = 0.05
 TIE_F16 = 1e-3  # one fp16 step of a score near 1 (2^-10)
