@@ -962,9 +962,10 @@ def main():
             "encoder": {"ms": sum(enc_ms) / len(enc_ms),
                         "achieved_gbs": enc_bytes / (sum(enc_ms) / len(enc_ms) * 1e-3) / 1e9,
                         "peak_gbs": pk["hbm_gbs"],
-                        "note": "ms / achieved_gbs: in the timed step, right after the fused kernel (its "
-                                "power-capped clock); alone_*: 10 launches after the timed region, L2 "
-                                "flushed before each",
+                        "note": "ms / achieved_gbs: in the timed step, launched after the host read the "
+                                "previous step's kernel times (the GPU idles for that gap, and a sub-ms "
+                                "kernel after an idle gap runs partly below the clock it had); alone_*: "
+                                "10 launches after the timed region, each right behind an L2 flush",
                         "alone_ms": sum(enc_alone) / len(enc_alone),
                         "alone_gbs": enc_bytes / (sum(enc_alone) / len(enc_alone) * 1e-3) / 1e9},
             "kernels_ms": {"gemm_topk": g_avg, "merge": sum(merge_ms) / len(merge_ms),
