@@ -134,8 +134,9 @@ typedef struct {
                       reserved[1]: kernel, 0 auto (CTA pairs above 128 reads),
                       1 single-CTA, 2 CTA-pair;
                       reserved[2]: epilogue form of either kernel, 0 auto
-                      (8 warps for work units of at most 8192 column tiles,
-                      else 4), 1 four warps, 2 eight warps (k <= 32);
+                      (CTA-pair kernel: 8 warps for k <= 32; single-CTA
+                      kernel: 8 warps for work units of at most 8192 column
+                      tiles, else 4), 1 four warps, 2 eight warps (k <= 32);
                       reserved[3]: pacing of the CTA-pair kernel, 0 default
                       (a pair naps while it is more than 16 column tiles
                       ahead of the slowest pair, so the pairs share index
