@@ -22,12 +22,15 @@ paths relative to the q4bio-qpg/qpg-rotormap tree):
 C restatements (oracle/rotormap_oracle.c, built by oracle/Makefile):
   rope_f64 / rope_f32 / f32_to_e4m3 / f32_to_f16 / topk_e4m3 / scores_e4m3.
 
-Parity status: "parity unpinned" in the strict sense -- the reference (Julia)
-cannot run in this container and commits no golden input/output vectors; the
-oracle is pinned by the reference's own known-answer properties, hand-derived
-vectors (tests/golden/), and the reference's committed experiment curves
-(tests/golden/rope_mutation_sweep_bins.json: the shift-sweep anchor matched to
-1e-4, the mutation-sweep curve within the fragment-to-fragment spread).
+Parity status: pinned against the reference's own outputs.  The reference
+(Julia) cannot run here, but it commits three encoder sweep curves
+(RotorMap/experiments/out/rope_*_sweep.csv: its fp64 encoder at k = 20,000,
+s5 m1 c5, on fixtures drawn from Julia's Xoshiro).  rotormap.jlrandom
+reproduces those fixtures draw for draw, and rope_f64 reproduces the
+curves' float64 inner products to within 1e-12 (observed <= 7e-16;
+tests/golden/rope_sweeps.json, tests/test_cpu_oracle.py).  The reference's
+known-answer properties and hand-derived vectors (tests/golden/) cover the
+rest (s > c scramble, m > 1, quantisation, top-k).
 """
 from __future__ import annotations
 

@@ -1,9 +1,11 @@
 """Seeded synthetic genomes and reads (stand-ins for the reference's fixture
 generators in RotorMap/common/dna.jl and RotorMap/reads/sample.jl).
 
-The reference draws its fixtures from Julia's Xoshiro stream, which is not
-reproducible here; these generators keep the same shapes and models with
-numpy's PCG64:
+The reference draws its fixtures from Julia's Xoshiro stream;
+rotormap.jlrandom reproduces those draws exactly (generate_reference,
+mutate, mutate_shift) for fixtures that must equal the reference's.  The
+workload generators here keep the reference's shapes and models at any
+size with numpy's PCG64:
   * genome: iid bases with a GC fraction, optional N runs (lengths uniform
     in [run_min, run_max]) covering a given fraction of the bases;
   * `:even` read sampling over each record's N-free windows, midpoints of

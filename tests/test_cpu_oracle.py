@@ -118,13 +118,20 @@ def test_topk_oracle_orders_ties_by_column():
 
 
 # ------------------------------------------------ the reference's own experiment outputs
-# RotorMap/experiments/rope_mutation_sweep.jl and rope_shift_mutation_sweep.jl
-# ran the reference's fp64 encoder (k = 20,000, s5 m1 c5, normalize 0) and
-# committed their curves; tests/golden/make_sweep_bins.py keeps per-bin
-# statistics and the shift sweep's anchor row.
+# RotorMap/experiments/rope_{mutation,double_mutation,shift_mutation}_sweep.jl
+# ran the reference's fp64 encoder (k = 20,000, s5 m1 c5, normalize 0) on
+# Julia-seeded fixtures and committed their curves;
+# tests/golden/make_sweep_golden.py copies them into rope_sweeps.json.
+# rotormap.jlrandom draws the same fixtures (Julia's Xoshiro stream, the
+# reference's generate_reference / mutate / mutate_shift), so the oracle is
+# compared with the reference's own float64 results value for value.
 
-SWEEP = json.loads((Path(__file__).parent / "golden" / "rope_mutation_sweep_bins.json").read_text())
+SWEEPS = json.loads((Path(__file__).parent / "golden" / "rope_sweeps.json").read_text())
 SK, SS, SM, SC = 20000, 5, 1, 5
+# the curves are float64 results of the same arithmetic; 1e-12 absolute is
+# ~5,000 ulp at these magnitudes, while a fixture that differs in a single
+# base moves an inner product by ~1e-4
+PIN_ATOL = 1e-12
 
 
 def _pack(codes_list):
@@ -133,53 +140,87 @@ def _pack(codes_list):
 
 
 def _ip(e0, e1):
-    """(Re<z0,z1>, |<z0,z1>|) of two split [Re; Im] unit vectors."""
+    """(Re<z0,z1>, |<z0,z1>|) of two split [Re; Im] unit vectors
+    (rope_inner, RotorMap/experiments/rope_mutation_sweep.jl:67-73)."""
     D = e0.size // 2
     re_ = float(e0 @ e1)
     im = float(e0[:D] @ e1[D:] - e0[D:] @ e1[:D])
     return re_, math.hypot(re_, im)
 
 
-def test_shift_anchor_of_the_reference_sweep():
-    """The shift sweep's anchor (pristine fragment vs the same fragment moved
-    by 500 bases) is reproduced to 1e-4 on random fragments when the moved-out
-    head re-enters as the tail (a rotation: every window keeps its s-mer and
-    only its phase turns by theta*500).  This pins theta = 2*pi/k, the window
-    count k - s + 1, the G-bin zeroing and the unit normalisation.  (With a
-    random tail instead -- the committed mutate_shift -- the same encoder
-    gives ip_re ~0.962 / ip_abs ~0.975: the committed curve was made with the
-    rotation.)"""
-    a = SWEEP["shift_anchor"]
-    for seed in (1, 2, 3):
-        frag = np.random.default_rng(seed).integers(0, 4, SK).astype(np.uint8)
-        e, _ = orc.rope_f64(_pack([frag, np.roll(frag, -a["shift"])]), SK, SS, SM, SC)
-        ip_re, ip_abs = _ip(e[0], e[1])
-        assert abs(ip_re - a["ip_re"]) < 1e-4 and abs(ip_abs - a["ip_abs"]) < 1e-4
+def _fragment():
+    from rotormap import jlrandom
+    f = SWEEPS["fragment"]
+    return jlrandom.generate_reference(f["n"], f["seed"])
 
 
-def test_mutation_sweep_curve_of_the_reference():
-    """The mutation sweep restated with numpy draws: a random fragment,
-    mutate_edits (the reference's edit model) at the reference's error-rate
-    grid, the oracle's fp64 encoder.  The committed curve comes from one
-    Julia-seeded fragment, so only the shape is comparable: every 20-bin mean
-    lies within 0.04 of the reference's (fragment-to-fragment spread of the
-    mean offset measured over 24 fragments: +0.015 +- 0.0065), and the curve
-    falls monotonically like the reference's."""
-    from rotormap import synth
-    rng = np.random.default_rng(42)
-    frag = rng.integers(0, 4, SK).astype(np.uint8)
-    errs = 0.5 * np.arange(1000) / 999
-    idx = np.arange(0, 1000, 4)
-    muts = [frag] + [synth.mutate_edits(frag, errs[i], np.random.default_rng(1000 + i)) for i in idx]
+def _pre(frag, name):
+    from rotormap import jlrandom
+    pre = SWEEPS["sweeps"][name]["pre"]
+    if pre is None:
+        return frag
+    rng = jlrandom.Xoshiro(pre["seed"])
+    if pre["kind"] == "mutate":
+        return jlrandom.mutate(frag, pre["err"], rng)
+    return jlrandom.mutate_shift(frag, pre["err"], rng)
+
+
+def _check_rows(name, stride):
+    from rotormap import jlrandom
+    frag = _fragment()
+    pre = _pre(frag, name)
+    rows = SWEEPS["sweeps"][name]["rows"]
+    rows = rows[::stride] + ([rows[-1]] if (len(rows) - 1) % stride else [])
+    base = SWEEPS["copy_seed_base"]
+    muts = [frag] + [jlrandom.mutate(pre, err, jlrandom.Xoshiro(base + i)) for i, err, _, _ in rows]
     assert all(m.size == SK for m in muts)
     e, _ = orc.rope_f64(_pack(muts), SK, SS, SM, SC)
-    ips = np.array([_ip(e[0], x) for x in e[1:]])
-    err = errs[idx]
-    means = []
-    for b in SWEEP["bins"]:
-        sel = (err >= b["err_lo"]) & ((err < b["err_hi"]) if b["err_hi"] < 0.5 else (err <= b["err_hi"]))
-        m_re, m_abs = ips[sel, 0].mean(), ips[sel, 1].mean()
-        assert abs(m_re - b["ip_re_mean"]) < 0.04 and abs(m_abs - b["ip_abs_mean"]) < 0.04
-        means.append(m_re)
-    assert all(np.diff(means) < 0)
-    assert np.all(ips[:, 1] >= ips[:, 0] - 1e-12)
+    worst = 0.0
+    for j, (i, err, ip_re, ip_abs) in enumerate(rows):
+        got = _ip(e[0], e[j + 1])
+        worst = max(worst, abs(got[0] - ip_re), abs(got[1] - ip_abs))
+    assert worst < PIN_ATOL, f"{name} sweep: largest difference {worst:.3e}"
+    return len(rows)
+
+
+def test_julia_stream_restatement():
+    """Julia's Xoshiro draws as the reference's fixtures use them: the
+    shift sweep's pre-mutation draws its 500-base tail from Xoshiro(42), the
+    generator that made the fragment, so the tail is the fragment's own head
+    and the shifted copy is a rotation."""
+    from rotormap import jlrandom
+    frag = _fragment()
+    assert frag.size == SK and set(np.unique(frag)) <= {0, 1, 2, 3}
+    assert np.array_equal(jlrandom.mutate_shift(frag, 0.05, jlrandom.Xoshiro(42)), np.roll(frag, -500))
+    # mutate keeps the length; err = 0 is the identity
+    assert np.array_equal(jlrandom.mutate(frag, 0.0, jlrandom.Xoshiro(43)), frag)
+    m = jlrandom.mutate(frag, 0.25, jlrandom.Xoshiro(7))
+    assert m.size == SK and 0.4 < float(np.mean(m != frag)) < 0.9
+    # the error grid of the sweeps
+    errs = [r[1] for r in SWEEPS["sweeps"]["mutation"]["rows"]]
+    assert np.array_equal(np.array(errs), jlrandom.sweep_errs(1000))
+
+
+def test_shift_anchor_of_the_reference_sweep():
+    """The shift sweep's err = 0 row (fragment vs its 500-base shift) to
+    within PIN_ATOL of the reference's float64 value."""
+    row = SWEEPS["sweeps"]["shift"]["rows"][0]
+    assert row[1] == 0.0
+    frag = _fragment()
+    e, _ = orc.rope_f64(_pack([frag, _pre(frag, "shift")]), SK, SS, SM, SC)
+    got = _ip(e[0], e[1])
+    assert abs(got[0] - row[2]) < PIN_ATOL and abs(got[1] - row[3]) < PIN_ATOL
+
+
+def test_mutation_sweep_of_the_reference():
+    """Every 8th row of the single-mutation sweep (and its last) equals the
+    reference's float64 inner products."""
+    assert _check_rows("mutation", 8) >= 125
+
+
+@pytest.mark.parametrize("name", ["double", "shift"])
+def test_pre_mutated_sweeps_of_the_reference(name):
+    """The double-mutation sweep (0.3 pre-mutation by mutate) and the shift
+    sweep (0.05 pre-shift by mutate_shift): every other kept row equals the
+    reference's float64 inner products."""
+    assert _check_rows(name, 2) >= 50

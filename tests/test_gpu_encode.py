@@ -175,24 +175,23 @@ def test_ref_windows_columns_match_oracle():
 
 def test_reference_experiment_curves_through_the_gpu_encoder():
     """The reference's committed experiment outputs (k = 20,000, s5 m1 c5;
-    tests/golden/rope_mutation_sweep_bins.json) reproduced by the GPU
-    encoder's fp32 output: the 500-base rotation anchor of the shift sweep
-    to 1e-4, and mutation-sweep inner products equal to the oracle's fp64
-    ones within 1e-5 (the curve itself is checked against the reference's
-    on the CPU)."""
+    tests/golden/rope_sweeps.json) reproduced by the GPU encoder's fp32 rows
+    on the same Julia-seeded fixtures (rotormap.jlrandom): the shift
+    sweep's anchor and 21 mutation-sweep points within 1e-5 of the
+    reference's float64 inner products."""
     import json
     from pathlib import Path
-    from rotormap import synth
-    sweep = json.loads((Path(__file__).parent / "golden" / "rope_mutation_sweep_bins.json").read_text())
+    from rotormap import jlrandom, synth
+    sw = json.loads((Path(__file__).parent / "golden" / "rope_sweeps.json").read_text())
     K, S, M, C = 20000, 5, 1, 5
     re = rm.RopeEncoder(k=K, s=S, m=M, c=C)
-    frag = np.random.default_rng(5).integers(0, 4, K).astype(np.uint8)
-    errs = 0.5 * np.arange(1000) / 999
-    muts = [frag, np.roll(frag, -sweep["shift_anchor"]["shift"])]
-    muts += [synth.mutate_edits(frag, errs[i], np.random.default_rng(i)) for i in range(0, 1000, 50)]
+    frag = jlrandom.generate_reference(sw["fragment"]["n"], sw["fragment"]["seed"])
+    shifted = jlrandom.mutate_shift(frag, 0.05, jlrandom.Xoshiro(42))
+    rows = sw["sweeps"]["mutation"]["rows"][::50] + [sw["sweeps"]["mutation"]["rows"][-1]]
+    muts = [frag, shifted] + [jlrandom.mutate(frag, err, jlrandom.Xoshiro(sw["copy_seed_base"] + i))
+                              for i, err, _, _ in rows]
     words = synth.pack_reads(muts, K)
     g, _ = _gpu_encode(words, re)
-    o, _ = orc.rope_f64(words, K, S, M, C)
     D = g.shape[1] // 2
 
     def ip(a, b):
@@ -201,10 +200,10 @@ def test_reference_experiment_curves_through_the_gpu_encoder():
         r = a @ b
         return r, np.hypot(r, a[:D] @ b[D:] - a[D:] @ b[:D])
 
-    sr, sa = ip(g[0], g[1])
-    assert abs(sr - sweep["shift_anchor"]["ip_re"]) < 1e-4 and abs(sa - sweep["shift_anchor"]["ip_abs"]) < 1e-4
-    for j in range(2, len(muts)):
-        assert np.allclose(ip(g[0], g[j]), ip(o[0], o[j]), rtol=0, atol=1e-5)
+    anchor = sw["sweeps"]["shift"]["rows"][0]
+    assert np.allclose(ip(g[0], g[1]), anchor[2:], rtol=0, atol=1e-5)
+    for j, (_, _, ip_re, ip_abs) in enumerate(rows):
+        assert np.allclose(ip(g[0], g[j + 2]), (ip_re, ip_abs), rtol=0, atol=1e-5)
 
 
 SPARSE_CONFIGS = [(150, 8, 4, 4), (100, 8, 4, 4), (250, 8, 4, 4), (37, 5, 1, 3), (20, 8, 2, 2), (60, 6, 8, 3)]
