@@ -1027,7 +1027,7 @@ __global__ void __launch_bounds__(256) k_encode_sparse(EncParams P, const uint32
 }
 
 template <int OUT, int M>
-__global__ void __launch_bounds__(256) k_encode_sparse_ref(EncParams P, const uint32_t *__restrict__ genome,
+__global__ void __launch_bounds__(256, M <= 4 ? 4 : 1) k_encode_sparse_ref(EncParams P, const uint32_t *__restrict__ genome,
                                                            const int64_t *__restrict__ win_pos, int64_t nwin,
                                                            int64_t batch, void *dest, float *norms,
                                                            float *scales) {
