@@ -133,13 +133,24 @@ def mutate_edits(codes: np.ndarray, err: float, rng) -> np.ndarray:
 def sample_reads_even(heads, recs, n: int, k: int, err: float = 0.0, seed: int = 42,
                       model: str = "subs"):
     """`:even` draw over the N-free pool (sample.jl:566-582) -> (reads codes
-    list, provenance headers, record index, 1-based starts)."""
+    list, provenance headers, record index, 1-based starts).
+
+    model "subs": iid substitutions at rate err (numpy draws); "mutate": the
+    reference's edit model with numpy draws; "reference": the reference
+    sampler's own draws (sample.jl:589-604): `Xoshiro(seed)`, one child
+    generator per read seeded by `rand(rng, Int64)`, and `mutate` on that
+    child (rotormap.jlrandom) -- the reads `sample_reads(...; draw = :even,
+    err, seed)` returns for the same records."""
     pools = [_nfree_window_starts(nm, k) for _, nm in recs]
     w = np.array([p.size for p in pools], np.int64)
     if w.sum() == 0:
         raise ValueError(f"no N-free k = {k} window")
     alloc = even_alloc(w, n)
     rng = np.random.default_rng(seed)
+    if model == "reference":
+        from . import jlrandom
+        jl = jlrandom.Xoshiro(seed)
+        children = [jlrandom.Xoshiro(jl.rand_i64()) for _ in range(n)]
     reads, hd, rix, starts = [], [], [], []
     i = 0
     for j, nj in enumerate(alloc):
@@ -150,6 +161,8 @@ def sample_reads_even(heads, recs, n: int, k: int, err: float = 0.0, seed: int =
             codes = recs[j][0][st0:st0 + k]
             if model == "subs":
                 codes = substitute(codes, err, rng)
+            elif model == "reference":
+                codes = jlrandom.mutate(codes, err, children[i])
             else:
                 codes = mutate_edits(codes, err, rng)
             i += 1

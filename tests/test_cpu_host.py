@@ -269,6 +269,29 @@ def test_synth_even_sampler_and_packing():
     assert abs((mutated != 0).mean() - 0.05) < 0.005
 
 
+def test_even_sampler_with_the_reference_draws():
+    """model="reference": the reference sampler's draws (sample.jl:589-604):
+    Xoshiro(seed), one child per read seeded by rand(rng, Int64), mutate on
+    the child -- deterministic in the seed, length kept, err = 0 exact
+    windows, and read i equal to mutate(window_i) on child i."""
+    from rotormap import jlrandom
+    heads = [">g1 a", ">g2 b"]
+    recs = synth.random_genome([5000, 3000], seed=1)
+    r0, hd0, rix, st = synth.sample_reads_even(heads, recs, 40, 150, 0.0, seed=5, model="reference")
+    for r, j, s0 in zip(r0, rix, st):
+        assert np.array_equal(r, recs[j][0][s0 - 1:s0 - 1 + 150])
+    r5, hd5, _, _ = synth.sample_reads_even(heads, recs, 40, 150, 0.05, seed=5, model="reference")
+    again, _, _, _ = synth.sample_reads_even(heads, recs, 40, 150, 0.05, seed=5, model="reference")
+    other, _, _, _ = synth.sample_reads_even(heads, recs, 40, 150, 0.05, seed=6, model="reference")
+    assert hd5 == hd0 and all(r.size == 150 for r in r5)
+    assert all(np.array_equal(a, b) for a, b in zip(r5, again))
+    assert not all(np.array_equal(a, b) for a, b in zip(r5, other))
+    rng = jlrandom.Xoshiro(5)
+    kids = [jlrandom.Xoshiro(rng.rand_i64()) for _ in range(40)]
+    for i in (0, 17, 39):
+        assert np.array_equal(r5[i], jlrandom.mutate(r0[i], 0.05, kids[i]))
+
+
 def test_mutate_edits_follows_the_reference_model():
     """mutate (RotorMap/common/dna.jl:120-183): ceil(n*err) operations split
     floor(n_err/3) insertions, as many deletions, the rest substitutions; the

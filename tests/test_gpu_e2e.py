@@ -33,8 +33,8 @@ def fixture():
     return heads, recs, re, idx
 
 
-def _reads_file(tmp_path, heads, recs, n, err, seed, name):
-    reads, hd, _, _ = synth.sample_reads_even(heads, recs, n, K, err, seed=seed)
+def _reads_file(tmp_path, heads, recs, n, err, seed, name, model="subs"):
+    reads, hd, _, _ = synth.sample_reads_even(heads, recs, n, K, err, seed=seed, model=model)
     p = tmp_path / name
     p.write_bytes(synth.reads_fasta(hd, reads))
     return p, reads, hd
@@ -59,6 +59,17 @@ def test_selftest_err0_all_map_at_rank1(fixture, tmp_path):
 def test_selftest_err5_top20_floor(fixture, tmp_path):
     heads, recs, re, idx = fixture
     p, _, _ = _reads_file(tmp_path, heads, recs, 200, 0.05, 7, "r5.fa")
+    r = rm.map_and_count(re, str(p), idx, ktop=20)
+    assert r["total"] == 200 and r["correct"] / 200 >= 0.90
+
+
+def test_selftest_err5_floor_with_the_reference_sampler(fixture, tmp_path):
+    """The self-test's mutated reads as the reference samples them: its
+    edit model (substitutions, insertions, deletions) on its own Xoshiro
+    draws (rotormap.jlrandom), 200 reads at err = 0.05, floor 0.90
+    (RotorMap/selftest.jl:62-63, 204-222)."""
+    heads, recs, re, idx = fixture
+    p, _, _ = _reads_file(tmp_path, heads, recs, 200, 0.05, 11, "r5ref.fa", model="reference")
     r = rm.map_and_count(re, str(p), idx, ktop=20)
     assert r["total"] == 200 and r["correct"] / 200 >= 0.90
 
