@@ -282,6 +282,8 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0)
     eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=65536, score="f16")
     srv = serving.MappingServer(eng, re)
     srv.submit(reqs[0][:64]).result(300)  # warm-up
+    clk = Clocks(dev.index if dev.index is not None else 0)
+    clk.start()
     t0 = time.perf_counter()
     wait = replay(t0)
     hs = []
@@ -290,12 +292,20 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0)
         hs.append(srv.submit(w, t_arrival=t0 + a))
     res = [h.result(600) for h in hs]
     done_times = [h.t_done for h in hs]  # results in host memory (CLOCK_MONOTONIC = perf_counter's clock)
+    clocks = clk.stop()
     sst = srv.stats()
     srv.close()
     out["serving"] = stats(done_times, t0)
     out["serving"]["batches"] = sst.batches
     out["serving"]["loop"] = "native (r2m_server_*)"
     out["serving"]["tflops"] = total * flop_per_read / out["serving"]["span_s"] / 1e12
+    # tensor-pipe utilisation over the whole span (arrival gaps, encodes and
+    # merges included): achieved / (16384 dense fp8 FLOP per SM per clock x
+    # SMs x the median SM clock sampled during the span)
+    out["serving"]["clocks"] = clocks
+    if clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        out["serving"]["tensor_pipe_est"] = out["serving"]["tflops"] / (16384.0 * sms * clocks["sm_mhz"] * 1e-6)
     # plain batch path, reference engine structure (cuBLASLt fp8 + segmented top-k, batch 8192)
     peng = rm.PlainEngine(idx.embeds8, k=TOPK, w=65536, rows_cap=8192)
     serving.plain_map(peng, re, [(0.0, reqs[0][:64])], batch=8192)
@@ -756,7 +766,9 @@ def summary(line: dict) -> dict:
                              "vs_plain_fused_kernel": _r(sv["serving"]["reads_per_s"] /
                                                          sv["plain_fused_kernel"]["reads_per_s"], 3),
                              "recall_vs_plain_ties": _r(sv["top20_recall_vs_plain_reference"], 6),
-                             "untied_misses": sv["untied_misses"], "reads": sv["reads"]}
+                             "untied_misses": sv["untied_misses"], "reads": sv["reads"],
+                             "tflops": _r(sv["serving"]["tflops"]),
+                             "tensor_pipe_est": _r(sv["serving"].get("tensor_pipe_est"), 3)}
         if sv.get("fp64_check"):
             out["C4_serving"]["fp64_recall"] = _r(sv["fp64_check"]["top20_recall_fp8_vs_fp64"], 4)
             out["C4_serving"]["fp64_err_max"] = _r(sv["fp64_check"]["score_abs_err_fp8"]["max"], 3)
