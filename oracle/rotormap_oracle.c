@@ -5,15 +5,16 @@
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg compare the CUDA
  * library against; nothing in the product path links or calls it.
  *
- * Parity status: the reference is Julia (not installed here) and commits no
- * golden vectors, so this restatement is pinned by the reference's own
- * known-answer properties (unit energy, window / reverse-complement word
- * identities, e4m3 == host conversion, exact top-k multisets) and by the
- * hand-derived vectors under tests/golden/, and by curves the reference's
- * own fp64 encoder produced and committed (its experiment outputs at k =
- * 20,000, s5 m1 c5: tests/golden/rope_mutation_sweep_bins.json) -- not by
- * input/output vectors of the reference ("parity unpinned" in the strict
- * sense).
+ * Parity status: pinned against the reference's own outputs.  The
+ * reference (Julia, not installed here) commits three encoder sweep curves
+ * (RotorMap/experiments/out/rope_*_sweep.csv: its fp64 encoder at k =
+ * 20,000, s5 m1 c5, on Julia-Xoshiro fixtures); with the same fixtures drawn
+ * here (rotormap.jlrandom), orc_rope_frag_f64 reproduces their float64 inner
+ * products to within 1e-12 (tests/golden/rope_sweeps.json).  The
+ * reference's known-answer properties (unit energy, window /
+ * reverse-complement word identities, e4m3 == host conversion, exact top-k
+ * multisets) and the hand-derived vectors under tests/golden/ cover what
+ * those curves do not exercise (the scramble at s > c, m > 1).
  *
  * Functions and the reference code each one restates:
  *   orc_rope_frag_f64   _ref_rope_frag / _ref_rope_frag_real
