@@ -231,12 +231,14 @@ def fp64_check(re, idx, genome_dev, words_dev, locs8, vals8, n_sample: int, seed
 # ---------------------------------------------------------------- serving leg
 
 
-def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0):
+def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0, kernel_tflops=None):
     """Serving form vs the plain batch path at human-scale geometry: 3.1 Gbp
     genome of 24 records (lengths U[50, 250] Mbp rescaled, GC 41%, 5% N runs),
     fwd + rc windows at k = 150, kstep = 1880 -> ~3.3M columns (~6.3 GiB e4m3),
     Poisson arrivals of requests of U{1..100,000} reads with substitution
-    rates U[0, 0.10].  Same arrival schedule for every path."""
+    rates U[0, 0.10], offered at 1.5x the fused kernel's capacity (the
+    headline leg's measured TFLOP/s when given, else 2.2 PFLOP/s), so the
+    server stays loaded.  Same arrival schedule for every path."""
     import torch
     import rotormap as rm
     from rotormap import serving, synth
@@ -255,9 +257,10 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0)
         truth.append((recs, offs))
     torch.cuda.empty_cache()
     total = int(sizes.sum())
-    # arrivals: Poisson, mean gap = mean request / (1.5 x a fused-kernel capacity estimate)
+    # arrivals: Poisson, mean gap = mean request / (1.5 x the fused kernel's capacity)
     flop_per_read = 2.0 * re.rdim * idx.N
-    cap_est = 2.2e15 / flop_per_read
+    cap_flops = kernel_tflops * 1e12 if kernel_tflops else 2.2e15
+    cap_est = cap_flops / flop_per_read
     gaps = rng.exponential(float(sizes.mean()) / (1.5 * cap_est), n_requests)
     arrivals = np.concatenate([[0.0], np.cumsum(gaps[1:])])
 
@@ -276,7 +279,8 @@ def serving_leg(dev, n_requests: int = 16, seed: int = 31, fp64_sample: int = 0)
 
     out = {"workload": f"3.1 Gbp genome (24 records, GC 41%, 5% N), k=150 kstep=1880 -> N={idx.N} "
                        f"columns ({idx.N * re.rdim / 2**30:.2f} GiB e4m3), {n_requests} Poisson requests "
-                       f"of U{{1..100000}} reads (total {total}), subs U[0,0.10], top-20, f16 scores",
+                       f"of U{{1..100000}} reads (total {total}), subs U[0,0.10], top-20, f16 scores, "
+                       f"offered at 1.5 x {cap_flops / 1e15:.2f} PFLOP/s",
            "index_cols": idx.N, "requests": n_requests, "reads": total}
     # serving form (fused kernel, continuous batching)
     eng = rm.TopKEngine(idx.embeds8, k=TOPK, rows_cap=65536, score="f16")
@@ -997,7 +1001,8 @@ def main():
     torch.cuda.empty_cache()
     if rank == 0:
         if world == 1 and not args.no_serving:
-            line["serving"] = serving_leg(dev, args.requests, fp64_sample=args.fp64_sample)
+            line["serving"] = serving_leg(dev, args.requests, fp64_sample=args.fp64_sample,
+                                          kernel_tflops=line["roofline"]["achieved"] if "roofline" in line else None)
         if world == 1 and not args.no_precision:
             line["precision"] = precision_leg(dev, args.precision_reads, args.precision_sample)
         if world == 1 and not args.no_batching:
