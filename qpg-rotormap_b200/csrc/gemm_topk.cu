@@ -27,6 +27,7 @@
 #include <float.h>
 #include <limits.h>
 
+#include <cmath>
 #include <mutex>
 #include <vector>
 
@@ -888,18 +889,41 @@ static size_t gemm_smem_bytes(int H) {
          (size_t)(epi_threads(H) - 64) * SCRATCH_F * sizeof(float);
 }
 
-// Column splits for a given number of read tiles: enough units to keep
-// every CTA busy, chosen to minimise the last-wave imbalance.
-static int choose_splits(int m_tiles, int n_tiles, int ctas, int forced, int max_splits = MAX_SPLITS) {
+// Column splits for a given number of read tiles.  The single-CTA kernel,
+// or fewer read tiles than half the CTA pairs: enough units to keep every
+// CTA busy, chosen to minimise the last-wave imbalance.  The CTA-pair kernel
+// with more read tiles runs power-bound, where a wave with a few idle pairs
+// loses little (the busy ones clock higher) but every doubling of the splits
+// costs about 9% at equal wave use (measured against 3,297,890 columns,
+// 16,384-65,536 reads: one split beat the imbalance-minimising choice by 8-18%
+// below 65,536 reads); so there the splits maximise
+// units / (waves x pairs) x 0.91^log2(splits) over 1..8.
+static int choose_splits(int m_tiles, int n_tiles, int ctas, int forced, int max_splits = MAX_SPLITS,
+                         bool pair = false) {
   if (forced > 0) {
     int s = forced;
     if (s > n_tiles) s = n_tiles;
     if (s > max_splits) s = max_splits;
     return s < 1 ? 1 : s;
   }
+  int cap = n_tiles < max_splits ? n_tiles : max_splits;
+  if (cap < 1) cap = 1;
+  if (pair && 2 * m_tiles >= ctas) {
+    int best = 1;
+    double best_score = -1.0;
+    for (int s = 1; s <= 8 && s <= cap; ++s) {
+      const long long units = (long long)m_tiles * s;
+      const long long waves = (units + ctas - 1) / ctas;
+      const double score = (double)units / (double)(waves * ctas) * std::pow(0.91, std::log2((double)s));
+      if (score > best_score + 1e-9) {
+        best_score = score;
+        best = s;
+      }
+    }
+    return best;
+  }
   int smin = (4 * ctas + m_tiles - 1) / m_tiles;
   if (smin < 1) smin = 1;
-  int cap = n_tiles < max_splits ? n_tiles : max_splits;
   if (smin > cap) smin = cap;
   int best = smin;
   double best_eff = -1.0;
@@ -1065,7 +1089,7 @@ static size_t lists_needed(int rows_cap, int n_tiles, int ctas, int forced, int 
     // either kernel may leave two partial lists per row and split
     (void)kind;
     const int H = KT <= 32 ? 2 : 1;
-    size_t l = (size_t)choose_splits(mt, n_tiles, c, forced, MAX_SPLITS / H) * H * mt * tile;
+    size_t l = (size_t)choose_splits(mt, n_tiles, c, forced, MAX_SPLITS / H, kind == 2) * H * mt * tile;
     if (l > lists) lists = l;
   }
   return lists;
@@ -1286,7 +1310,7 @@ extern "C" int r2m_batch_gemm_topk(r2m_engine *eng, const uint8_t *d_A, const fl
   g.N = eng->N;
   g.n_tiles = eng->n_tiles;
   const int hmax = eng->KT <= 32 ? 2 : 1;
-  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / hmax);
+  g.splits = choose_splits(g.num_m_tiles, eng->n_tiles, ctas_eff, eng->forced_splits, MAX_SPLITS / hmax, kind == 2);
   const int halves =
       eng->epi == 1 ? 1 : eng->epi == 2 ? hmax : epi_halves_for(kind, eng->KT, eng->n_tiles, g.splits);
   const int lists_per_row = halves * g.splits;  // partial lists each row leaves
@@ -1469,7 +1493,7 @@ extern "C" int r2m_batch_gemm_topk_noalloc(const uint8_t *d_B, const float *d_sc
   const int ctas_eff = kind == 2 ? (sms / 2 > 0 ? sms / 2 : 1) : sms;
   const int hmax = KT <= 32 ? 2 : 1;
   // the engine's automatic schedule, with the splits cut to the scratch
-  int splits = choose_splits(m_tiles, n_tiles, ctas_eff, 0, MAX_SPLITS / hmax);
+  int splits = choose_splits(m_tiles, n_tiles, ctas_eff, 0, MAX_SPLITS / hmax, kind == 2);
   int halves = epi_halves_for(kind, KT, n_tiles, splits);
   while (splits > 1 && (size_t)halves * splits * mpad > max_lists) {
     --splits;
