@@ -15,9 +15,10 @@ here:
     (rotl(s0 + s3, 23) + s0, then the standard state update);
     `rand(rng, Int64)` is the same 64 bits as a signed integer;
   * `rand(rng, Float64)`: (u >>> 11) * 2^-53;
-  * `rand(rng, collection)` of n elements: Lemire's nearly-divisionless
-    method on 1:n (64-bit product, the high word is the 0-based index, a
-    low word below (2^64 - n) mod n is redrawn).
+  * `rand(rng, collection)` of n elements, and `rand(rng, a:b)` of n
+    values (`0x00:0x03` included): Lemire's nearly-divisionless method on a
+    64-bit draw (64-bit product, the high word is the 0-based index, a low
+    word below (2^64 - n) mod n is redrawn).
 
 `mutate` goes through the reference's rope structure
 (RotorMap/common/treearrays.jl) with its leaf size of 1,000, so the edits
@@ -26,8 +27,10 @@ deletions that all fall in the left half: `deleteat!` hands them to the
 RIGHT child at the same offsets (treearrays.jl:152-153).
 
 These draws reproduce the reference's committed sweep curves
-(RotorMap/experiments/out/rope_*_sweep.csv) value for value; they are
-fixture generators, not part of the mapping path.
+(RotorMap/experiments/out/rope_*_sweep.csv) value for value, and the
+periodic-fragment table of RotorMap/legacy/test/ropeperiod.jl to its
+printed 6 decimals; they are fixture generators, not part of the mapping
+path.
 """
 from __future__ import annotations
 
@@ -221,6 +224,15 @@ def mutate_shift(dna, err: float, rng: Xoshiro, shift: int | None = None) -> np.
         shift = int(math.floor(n * err / 2))
     tail = np.array([rng.rand_index(4) for _ in range(shift)], np.uint8)
     return np.concatenate([dna[shift:], tail])
+
+
+def periodic_fragment(k: int, period: int, seed: int) -> np.ndarray:
+    """`periodic_fragment(k, p, seed)` (RotorMap/legacy/test/ropeperiod.jl):
+    a motif of `period` bases drawn by `rand(Xoshiro(seed), 0x00:0x03)`,
+    tiled to exactly k bases."""
+    rng = Xoshiro(seed)
+    motif = np.array([rng.rand_index(4) for _ in range(int(period))], np.uint8)
+    return motif[np.arange(int(k)) % int(period)]
 
 
 def sweep_errs(npts: int = 1000) -> np.ndarray:

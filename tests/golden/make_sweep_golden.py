@@ -20,10 +20,17 @@ other two.  Values are the CSVs' own decimal strings parsed as float64
 (Julia prints the shortest round-trip form, so they are the reference's
 exact float64 results).
 
+Also the RESULTS table of RotorMap/legacy/test/ropeperiod.jl (written in
+that file's header comment, 6 decimals): a 4,002-base motif drawn by
+`rand(Xoshiro(42), 0x00:0x03)` tiled to k = 20,000, the same fp64 encoder,
+copy i = mutate(fragment, 0.01 i; rng = Xoshiro(42 + i)), i = 1..50, plus
+the err = 0 row.
+
 Usage: python tests/golden/make_sweep_golden.py path/to/reference/checkout
 """
 import csv
 import json
+import re
 import sys
 from pathlib import Path
 
@@ -51,9 +58,22 @@ def main():
             "rows": [[i + 1, float(rows[i]["err"]), float(rows[i]["ip_re"]), float(rows[i]["ip_abs"])]
                      for i in keep],
         }
+    # the legacy periodic-fragment table: "err Re<IP> |IP|" rows, two per line
+    table = {}
+    pat = re.compile(r"#\s+(0\.\d\d)\s+(-?\d\.\d+)\s+(\d\.\d+)(?:\s+(0\.\d\d)\s+(-?\d\.\d+)\s+(\d\.\d+))?\s*$")
+    for line in open(Path(sys.argv[1]) / "RotorMap" / "legacy" / "test" / "ropeperiod.jl"):
+        m = pat.match(line)
+        if m:
+            for g in (1, 4):
+                if m.group(g):
+                    table[m.group(g)] = [float(m.group(g + 1)), float(m.group(g + 2))]
+    out["periodic"] = {"source": "RotorMap/legacy/test/ropeperiod.jl (RESULTS comment)", "k": 20000, "period": 4002,
+                       "seed": 42, "decimals": 6,
+                       "rows": [[int(round(float(e) * 100)), float(e), v[0], v[1]] for e, v in sorted(table.items())]}
     dst = Path(__file__).with_name("rope_sweeps.json")
     dst.write_text(json.dumps(out, separators=(",", ":")) + "\n")
-    print(f"wrote {dst} ({sum(len(s['rows']) for s in out['sweeps'].values())} rows)")
+    print(f"wrote {dst} ({sum(len(s['rows']) for s in out['sweeps'].values())} sweep rows, "
+          f"{len(out['periodic']['rows'])} periodic rows)")
 
 
 if __name__ == "__main__":

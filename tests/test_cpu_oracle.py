@@ -218,6 +218,25 @@ def test_mutation_sweep_of_the_reference():
     assert _check_rows("mutation", 8) >= 125
 
 
+def test_periodic_fragment_table_of_the_reference():
+    """The legacy periodic-fragment table (RotorMap/legacy/test/ropeperiod.jl:
+    a 4,002-base Xoshiro(42) motif tiled to k = 20,000, whose five copies
+    nearly cancel -- the phases are tested where the encoding is dominated
+    by a few hundred defect windows): all 51 rows within the table's printed
+    precision (6 decimals)."""
+    from rotormap import jlrandom
+    per = SWEEPS["periodic"]
+    frag = jlrandom.periodic_fragment(per["k"], per["period"], per["seed"])
+    rows = per["rows"]
+    muts = [frag] + [jlrandom.mutate(frag, err, jlrandom.Xoshiro(per["seed"] + i)) for i, err, _, _ in rows if i > 0]
+    e, _ = orc.rope_f64(_pack(muts), SK, SS, SM, SC)
+    got = [(1.0, 1.0)] + [_ip(e[0], x) for x in e[1:]]
+    half_ulp6 = 0.5e-6 + 1e-12
+    for (i, err, ip_re, ip_abs), g in zip(rows, got):
+        assert abs(g[0] - ip_re) <= half_ulp6 and abs(g[1] - ip_abs) <= half_ulp6, (err, g, ip_re, ip_abs)
+    assert abs(_ip(e[0], e[0])[0] - 1.0) < 1e-12
+
+
 @pytest.mark.parametrize("name", ["double", "shift"])
 def test_pre_mutated_sweeps_of_the_reference(name):
     """The double-mutation sweep (0.3 pre-mutation by mutate) and the shift
