@@ -127,7 +127,10 @@ typedef struct r2m_engine r2m_engine;
 
 /* Schedule knobs of the fused GEMM + top-k (0 = automatic). */
 typedef struct {
-  int splits;  /* column splits per read tile (k-split of the top-k) */
+  int splits;  /* column splits per read tile (k-split of the top-k); 0:
+                  the CTA-pair kernel with at least half the pairs' worth of
+                  read tiles takes 1..8 splits by wave use less ~9% per
+                  doubling, smaller batches enough for every CTA */
   int ctas;    /* persistent CTAs (default: SM count) */
   int reserved[6]; /* reserved[0] = 1: record CUDA events around the kernels
                       of every r2m_batch_gemm_topk (see r2m_engine_kernel_ms);
