@@ -1,6 +1,6 @@
 """Julia-exact fixture draws: the reference's `generate_reference`,
-`mutate` and `mutate_shift` (RotorMap/common/dna.jl) on the same random
-stream as Julia's `Random` standard library.
+`generate_reads`, `mutate` and `mutate_shift` (RotorMap/common/dna.jl) on
+the same random stream as Julia's `Random` standard library.
 
 The reference seeds every fixture with `Xoshiro(seed)` from Julia's
 `Random` stdlib (julia_version 1.12.2 in RotorMap/Manifest.toml; the stdlib
@@ -224,6 +224,23 @@ def mutate_shift(dna, err: float, rng: Xoshiro, shift: int | None = None) -> np.
         shift = int(math.floor(n * err / 2))
     tail = np.array([rng.rand_index(4) for _ in range(shift)], np.uint8)
     return np.concatenate([dna[shift:], tail])
+
+
+def generate_reads(dna_ref, k: int, n: int = 1, err: float = 0.15, seed: int = 0):
+    """`generate_reads(dna_ref, k, n; err, seed)` (RotorMap/common/dna.jl:
+    96-118): n 0-based window starts drawn by `rand(rng, 0:N-k, n)` from
+    `Xoshiro(seed)`, then one child generator per read seeded by
+    `rand(rng, Int64)`, and each read `mutate(window, err; rng = child)`.
+    Returns (reads, starts)."""
+    dna_ref = np.asarray(dna_ref, np.uint8)
+    N = int(dna_ref.size)
+    if k > N:
+        raise ValueError(f"k = {k} exceeds the reference length {N}")
+    rng = Xoshiro(seed)
+    pos = [rng.rand_index(N - k + 1) for _ in range(int(n))]
+    kids = [Xoshiro(rng.rand_i64()) for _ in range(int(n))]
+    reads = [mutate(dna_ref[p:p + k], err, kids[i]) for i, p in enumerate(pos)]
+    return reads, np.array(pos, np.int64)
 
 
 def periodic_fragment(k: int, period: int, seed: int) -> np.ndarray:

@@ -201,6 +201,26 @@ def test_julia_stream_restatement():
     assert np.array_equal(np.array(errs), jlrandom.sweep_errs(1000))
 
 
+def test_generate_reads_follows_the_reference_self_test():
+    """The reference self-test's stage A on Julia-exact draws
+    (RotorMap/selftest.jl:106-134): generate_reference(50_000; seed = 1);
+    generate_reads at err = 0 gives exact windows at 0-based starts in
+    0..N-k; mutate at err = 0 is the identity, and at err = 0.05 keeps the
+    length, changes bases and is deterministic in its generator."""
+    from rotormap import jlrandom
+    ref = jlrandom.generate_reference(50_000, 1)
+    assert ref.size == 50_000 and ref.max() <= 3
+    reads, pos = jlrandom.generate_reads(ref, 1_000, 64, err=0.0, seed=2)
+    assert len(reads) == 64 and pos.min() >= 0 and pos.max() <= 50_000 - 1_000
+    assert all(np.array_equal(r, ref[p:p + 1_000]) for r, p in zip(reads, pos))
+    assert np.array_equal(jlrandom.mutate(ref, 0.0, jlrandom.Xoshiro(3)), ref)
+    m1 = jlrandom.mutate(ref, 0.05, jlrandom.Xoshiro(4))
+    m2 = jlrandom.mutate(ref, 0.05, jlrandom.Xoshiro(4))
+    m3 = jlrandom.mutate(ref, 0.05, jlrandom.Xoshiro(5))
+    assert m1.size == ref.size and not np.array_equal(m1, ref)
+    assert np.array_equal(m1, m2) and not np.array_equal(m1, m3)
+
+
 def test_shift_anchor_of_the_reference_sweep():
     """The shift sweep's err = 0 row (fragment vs its 500-base shift) to
     within PIN_ATOL of the reference's float64 value."""
