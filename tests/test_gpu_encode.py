@@ -206,6 +206,34 @@ def test_reference_experiment_curves_through_the_gpu_encoder():
         assert np.allclose(ip(g[0], g[j + 2]), (ip_re, ip_abs), rtol=0, atol=1e-5)
 
 
+def test_reference_periodic_table_through_the_gpu_encoder():
+    """The reference's periodic-fragment table (RotorMap/legacy/test/
+    ropeperiod.jl, tests/golden/rope_sweeps.json: a 4,002-base Xoshiro(42)
+    motif tiled to k = 20,000, whose copies nearly cancel) through the GPU
+    encoder's fp32 rows on the Julia-exact fixtures: 11 of its rows within
+    1e-5 (the table prints 6 decimals)."""
+    import json
+    from pathlib import Path
+    from rotormap import jlrandom, synth
+    per = json.loads((Path(__file__).parent / "golden" / "rope_sweeps.json").read_text())["periodic"]
+    K = per["k"]
+    re = rm.RopeEncoder(k=K, s=5, m=1, c=5)
+    frag = jlrandom.periodic_fragment(K, per["period"], per["seed"])
+    rows = [r for r in per["rows"] if r[0] % 5 == 0 and r[0] > 0] + [per["rows"][1]]
+    muts = [frag] + [jlrandom.mutate(frag, err, jlrandom.Xoshiro(per["seed"] + i)) for i, err, _, _ in rows]
+    g, _ = _gpu_encode(synth.pack_reads(muts, K), re)
+    D = g.shape[1] // 2
+
+    def ip(a, b):
+        a = a.astype(np.float64)
+        b = b.astype(np.float64)
+        r = a @ b
+        return r, np.hypot(r, a[:D] @ b[D:] - a[D:] @ b[:D])
+
+    for j, (_, _, ip_re, ip_abs) in enumerate(rows):
+        assert np.allclose(ip(g[0], g[j + 1]), (ip_re, ip_abs), rtol=0, atol=1e-5)
+
+
 SPARSE_CONFIGS = [(150, 8, 4, 4), (100, 8, 4, 4), (250, 8, 4, 4), (37, 5, 1, 3), (20, 8, 2, 2), (60, 6, 8, 3)]
 
 
