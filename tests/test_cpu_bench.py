@@ -1,6 +1,7 @@
 """Pieces of bench.py's output contract that need no GPU: the roofline
 denominators (measured file or the stated fallback), the mapped-read share,
-and the reference arm under torchrun (ranks other than 0 exit 0 at once)."""
+the compact summary printed last, and the reference arm under torchrun
+(ranks other than 0 exit 0 at once)."""
 import json
 import os
 import subprocess
@@ -41,3 +42,21 @@ def test_reference_arm_other_ranks_exit_without_work():
                        capture_output=True, text=True, timeout=120, env=env, cwd=str(ROOT))
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+def test_summary_carries_every_leg_and_tolerates_missing_ones():
+    line = {"value": 42550.1, "e2e": {"value": 42410.2},
+            "roofline": {"achieved": 2925.3, "frac": 1.0569, "tensor_pipe": {"est_active_frac": 0.8042}},
+            "encoder": {"achieved_gbs": 510.2, "alone_gbs": 1193.0, "peak_gbs": 6547.8}}
+    out = bench.summary(line)
+    assert out["headline_reads_s"] == 42550.0 and out["tensor_pipe_est"] == 0.804
+    assert "C4_serving" not in out and "C2_precision" not in out
+    line["serving"] = {"serving": {"reads_per_s": 205595.3, "p50_s": 1.5805, "p99_s": 2.228, "tflops": 2777.2,
+                                   "tensor_pipe_est": 0.70222},
+                       "serving_vs_plain": 5.409, "plain_fused_kernel": {"reads_per_s": 156342.0},
+                       "top20_recall_vs_plain_reference": 1.0, "untied_misses": 0, "reads": 967725}
+    sv = bench.summary(line)["C4_serving"]
+    assert sv["tensor_pipe_est"] == 0.702 and sv["tflops"] == 2777.0 and sv["vs_plain_fused_kernel"] == 1.32
+    del line["serving"]["serving"]["tensor_pipe_est"]  # no clock samples: reported as null
+    assert bench.summary(line)["C4_serving"]["tensor_pipe_est"] is None
+    assert list(bench.summary(line))[-1] == "C4_serving"
